@@ -1,0 +1,133 @@
+# SPDX-License-Identifier: Apache-2.0
+"""TEST INFRASTRUCTURE ONLY: a ctypes wrapper of the CPU oracle (eda_oracle.cpp), the restatement of
+eda-cuda's decomposition that the tests, the smoke check and the benchmark's CPU baseline compare
+the CUDA path with. The product never imports this module.
+
+``decompose(x, max_imf=-1, tie_tolerance=None, sifts=3, check_finite=True, threads=1)`` takes a
+C-contiguous (B, *spatial) float32 or float64 array and returns ``(rows, info)`` with rows
+(B, P, *spatial) (P = 1 + the largest IMF count of the elements without an error, NaN rows for
+failed elements) and info the dict of the reference's native call (cpp/python/decompose.cpp:188-214):
+n_imfs, error, windows, sifts, spacing, energy (B, K), K the largest IMF count.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_lib = None
+
+
+def build() -> Path:
+    """Compiles the oracle (make) when the library is missing or older than its source."""
+    src = HERE / "eda_oracle.cpp"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(str(LIB))
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        f64p = ctypes.POINTER(ctypes.c_double)
+        L.eda_oracle_rows_cap.argtypes = [ctypes.c_int, i64p, ctypes.c_int32]
+        L.eda_oracle_rows_cap.restype = ctypes.c_int
+        L.eda_oracle_decompose.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64, i64p, ctypes.c_int32,
+            ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+            i32p, i32p, i32p, i32p, f64p, f64p, i32p, ctypes.c_char_p, ctypes.c_int64,
+        ]
+        L.eda_oracle_decompose.restype = ctypes.c_int
+        L.eda_oracle_rung_ladder.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, i32p]
+        L.eda_oracle_rung_ladder.restype = ctypes.c_int
+        L.eda_oracle_cube.argtypes = [ctypes.c_int, ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int32, ctypes.c_void_p]
+        L.eda_oracle_cube.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def rows_cap(shape: tuple[int, ...], max_imf: int = -1) -> int:
+    n = np.asarray(shape, dtype=np.int64)
+    return lib().eda_oracle_rows_cap(len(shape), _p(n, ctypes.c_int64), max_imf)
+
+
+def decompose_raw(x: np.ndarray, max_imf: int = -1, tie_tolerance: float | None = None, sifts: int = 3,
+                  check_finite: bool = True, threads: int = 1) -> tuple[np.ndarray, dict]:
+    """The oracle on (B, *spatial): rows (B, cap, *spatial) and the raw per-element arrays."""
+    x = np.ascontiguousarray(x)
+    assert x.dtype in (np.float32, np.float64) and 2 <= x.ndim <= 4
+    B, spatial = x.shape[0], x.shape[1:]
+    n = np.asarray(spatial, dtype=np.int64)
+    cap = rows_cap(spatial, max_imf)
+    rows = np.zeros((B, cap) + spatial, dtype=x.dtype)
+    he = cap - 1
+    n_imfs = np.zeros(B, np.int32)
+    error = np.zeros(B, np.int32)
+    exps = np.zeros(B, np.int32)
+    windows = np.zeros((B, he), np.int32)
+    sifts_out = np.zeros((B, he), np.int32)
+    spacing = np.zeros((B, he), np.float64)
+    energy = np.zeros((B, he), np.float64)
+    err = ctypes.create_string_buffer(512)
+    rc = lib().eda_oracle_decompose(
+        x.ctypes.data, 0 if x.dtype == np.float32 else 1, len(spatial), B, _p(n, ctypes.c_int64), max_imf,
+        -1.0 if tie_tolerance is None else float(tie_tolerance), sifts, int(bool(check_finite)), threads,
+        rows.ctypes.data, _p(n_imfs, ctypes.c_int32), _p(error, ctypes.c_int32), _p(windows, ctypes.c_int32),
+        _p(sifts_out, ctypes.c_int32), _p(spacing, ctypes.c_double), _p(energy, ctypes.c_double),
+        _p(exps, ctypes.c_int32), err, 512)
+    if rc != 0:
+        raise RuntimeError(f"oracle: {err.value.decode()}")
+    return rows, {"n_imfs": n_imfs, "error": error, "windows": windows, "sifts": sifts_out,
+                  "spacing": spacing, "energy": energy, "exp": exps}
+
+
+def decompose(x: np.ndarray, max_imf: int = -1, tie_tolerance: float | None = None, sifts: int = 3,
+              check_finite: bool = True, threads: int = 1) -> tuple[np.ndarray, dict]:
+    """The rows (B, P, *spatial) and the info dict of the reference's native call."""
+    rows, raw = decompose_raw(x, max_imf, tie_tolerance, sifts, check_finite, threads)
+    ok = raw["error"] == 0
+    P = int(raw["n_imfs"][ok].max(initial=-1)) + 1 if ok.any() else 1
+    P = max(P, 1)
+    K = int(raw["n_imfs"].max(initial=0))
+    info = {"n_imfs": raw["n_imfs"], "error": raw["error"]}
+    for name in ("windows", "sifts", "spacing", "energy"):
+        a = raw[name][:, :K].copy()
+        a[~ok] = 0
+        info[name] = a
+    out = rows[:, :P].copy()
+    return out, info
+
+
+def rung_ladder(d_min: float, d_max: float, w: int, n_max: int) -> list[int]:
+    out = np.zeros(32, np.int32)
+    k = lib().eda_oracle_rung_ladder(d_min, d_max, w, n_max, _p(out, ctypes.c_int32))
+    if k < 0:
+        raise ValueError("oracle: rung_ladder")
+    return [int(v) for v in out[:k]]
+
+
+def cube(f: np.ndarray, op: str, w: int) -> np.ndarray:
+    """One cube filter (op 'max', 'min' or 'box') of one element f (*spatial)."""
+    f = np.ascontiguousarray(f).copy()
+    n = np.asarray(f.shape, dtype=np.int64)
+    code = {"max": 0, "min": 1, "box": 3}[op]
+    lib().eda_oracle_cube(0 if f.dtype == np.float32 else 1, f.ndim, _p(n, ctypes.c_int64), code, w, f.ctypes.data)
+    return f
+
+
+def cores() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
