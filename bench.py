@@ -1,0 +1,300 @@
+# SPDX-License-Identifier: Apache-2.0
+"""Benchmark of the decomposition on B200: decompositions per second of the 2-D workload of 64
+float32 images of 512 x 512 (rings, wavy stripes, two Gaussian blobs and noise, seeded synthetic
+inputs with the shapes and value ranges of the workload), one decomposition call of the batch per
+step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank decomposes its own 64 images (weak scaling,
+no collective on the data path); the time of a step is the maximum over ranks. Prints one JSON line
+on rank 0:
+
+- value: decompositions/s with the inputs resident in HBM (CUDA events around each call, the L2
+  flushed between steps by writing a 256 MiB buffer);
+- e2e: the same through the public call with host input in pinned memory, the host-to-device copy
+  of the images and the device-to-host copy of the rows inside every step;
+- roofline: the dominant kernel (the cube-filter passes): its algorithmic bytes over its summed
+  CUDA-event time across the timed region against the measured copy bandwidth; traffic: DRAM bytes
+  per launch from the committed ncu summary (profiles/), when one exists;
+- cpu_baseline: the oracle (the CPU restatement of the method) on the host cores, one image per
+  thread.
+
+--impl reference times the reference's computation on the host cores: the reference ships no CPU
+implementation of the path and its GPU build needs its own CMake build with cuFFT, so this arm runs
+the oracle port of the same method (one image per host thread per step).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "eda-cuda_b200"))
+
+BATCH = 64
+SIDE = 512
+METRIC = "decompositions/s (2-D 64 x 512^2 float32, sifts 3)"
+UNIT = "decompositions/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "cube_pass_traffic.json"
+
+
+def workload(batch: int, seed: int) -> np.ndarray:
+    """The seeded synthetic images (batch, 512, 512) float32."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:SIDE, 0:SIDE].astype(np.float64)
+    out = np.empty((batch, SIDE, SIDE), np.float32)
+    stripes = 1.5 * np.cos(2 * np.pi * (x + 4 * np.sin(2 * np.pi * y / 128)) / 24)
+    for b in range(batch):
+        cy, cx = rng.uniform(0, SIDE, 2)
+        f = np.cos(2 * np.pi * np.hypot(y - cy, x - cx) / 6) + stripes
+        for _ in range(2):
+            by, bx = rng.uniform(0, SIDE, 2)
+            f = f + 3 * np.exp(-((y - by) ** 2 + (x - bx) ** 2) / (2 * 80.0**2))
+        f = f + 0.02 * rng.standard_normal((SIDE, SIDE))
+        out[b] = f.astype(np.float32)
+    return out
+
+
+def peak_hbm() -> tuple[float, str]:
+    if PEAKS.exists():
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and the throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            p = [v.strip() for v in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle(images: np.ndarray, threads: int) -> float:
+    """Seconds for the oracle to decompose `images` with `threads` host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    t0 = time.perf_counter()
+    oracle.decompose(images, threads=threads)
+    return time.perf_counter() - t0
+
+
+def host_cores() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def dist_env() -> tuple[int, int, int]:
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def run_reference(args) -> None:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cores = host_cores()
+    threads = max(1, min(cores, BATCH))
+    images = workload(threads, 1234)
+    for _ in range(args.warmup):
+        cpu_oracle(images, threads)
+    times = [cpu_oracle(images, threads) for _ in range(args.steps)]
+    value = threads * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"2-D {BATCH} x {SIDE}x{SIDE} float32 images (rings, wavy stripes, blobs, noise)",
+                   "sample_per_step": f"{threads} of the images, one per host thread"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{threads} images of {SIDE}x{SIDE} per step, one per thread; the reference has "
+                                   "no CPU implementation of the path, so the oracle port runs its method"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    import eda
+    from eda import _native
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        pg = dist
+    lib = _native.core()._lib
+    lib.eda_profile_read.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    x_host = workload(BATCH, 1000 + rank)
+    x_dev = torch.from_numpy(x_host).to(dev)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MiB > L2
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize(dev)
+
+    # warm-up (device input)
+    for _ in range(args.warmup):
+        eda.decompose(x_dev)
+    barrier()
+    # timed: device-resident inputs, events around each call, L2 flushed between calls
+    lib.eda_profile(1)
+    ms = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            y = eda.decompose(x_dev)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    launches, cl, cb, cms = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+    lib.eda_profile_read(ctypes.byref(launches), ctypes.byref(cl), ctypes.byref(cb), ctypes.byref(cms))
+    lib.eda_profile(0)
+    P = y.shape[1]
+    barrier()
+    total_ms = sum(ms)
+    if pg is not None:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = BATCH * world * args.steps / (total_ms / 1000.0)
+    # end to end: host input from pinned memory, rows back to the host, every step
+    pinned = torch.empty(x_host.shape, dtype=torch.float32).pin_memory()
+    pinned.numpy()[...] = x_host
+    xp = pinned.numpy()
+    e2e_ms = []
+    d2h = 0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        rows = eda.decompose(xp)
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+        d2h = rows.nbytes
+    e2e_total = sum(e2e_ms)
+    if pg is not None:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e = BATCH * world * args.steps / (e2e_total / 1000.0)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = max(1, min(host_cores(), BATCH))
+        secs = cpu_oracle(x_host[:threads], threads)
+        cpu = {"value": threads / secs, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{threads} of the {BATCH} images ({SIDE}x{SIDE} float32), one per host thread, "
+                         f"{secs:.1f} s"}
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    peak, peak_kind = peak_hbm()
+    achieved = (cb.value / (cms.value / 1000.0)) / 1e9 if cms.value > 0 else None
+    traffic = None
+    if TRAFFIC.exists():
+        traffic = json.loads(TRAFFIC.read_text()).get("dram_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"2-D {BATCH} x {SIDE}x{SIDE} float32 images per GPU (rings, wavy stripes, blobs, "
+                               "noise), sifts 3", "l2": "flushed between steps (256 MiB write)",
+                   "rows_per_element": int(P), "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "kernel": "cube_pass", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                     "traffic": traffic, "launches": int(cl.value),
+                     "share_of_step": (cms.value / total_ms) if total_ms else None},
+        "gpu_launches": int(launches.value),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+import ctypes  # noqa: E402
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

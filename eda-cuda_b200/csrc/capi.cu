@@ -1,0 +1,182 @@
+// SPDX-License-Identifier: Apache-2.0
+// The C ABI (include/eda_b200.h): exceptions become status codes and a per-thread message.
+#include "../../include/eda_b200.h"
+#include "driver.hpp"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+struct eda_run {
+  std::unique_ptr<edab::Run> run;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return EDA_OK;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return EDA_INVALID_ARGUMENT;
+  } catch (const edab::OutOfMemory& e) {
+    g_last_error = e.what();
+    return EDA_OUT_OF_MEMORY;
+  } catch (const std::bad_alloc& e) {
+    g_last_error = std::string("eda: host memory exhausted: ") + e.what();
+    return EDA_OUT_OF_MEMORY;
+  } catch (const edab::CudaError& e) {
+    g_last_error = e.what();
+    return e.code == cudaErrorMemoryAllocation ? EDA_OUT_OF_MEMORY : EDA_CUDA_ERROR;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return EDA_INTERNAL;
+  } catch (...) {
+    g_last_error = "eda: unknown failure";
+    return EDA_INTERNAL;
+  }
+}
+
+void put(char* buf, size_t len, const std::string& s) {
+  if (!buf || len == 0) return;
+  const size_t k = std::min(len - 1, s.size());
+  std::memcpy(buf, s.data(), k);
+  buf[k] = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int eda_decompose(const void* x, int x_on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                  const eda_params* params, void* stream, eda_run** out) {
+  return guarded([&] {
+    if (!out || !n || !params) throw std::invalid_argument("eda: null argument");
+    if (batch > 0 && !x) throw std::invalid_argument("eda: null input");
+    edab::Params p;
+    p.max_imf = params->max_imf;
+    p.tie_tolerance = params->tie_tolerance;
+    p.sifts = params->sifts;
+    p.check_finite = params->check_finite != 0;
+    p.max_chunk = params->max_chunk;
+    auto r = std::make_unique<eda_run>();
+    r->run = edab::decompose(x, x_on_device != 0, dtype, dim, batch, n, p, static_cast<cudaStream_t>(stream));
+    *out = r.release();
+  });
+}
+
+int eda_run_shape(const eda_run* run, int64_t* batch, int32_t* rows, int32_t* K, int64_t* count, int64_t* chunk) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("eda: null run");
+    const edab::Run& r = *run->run;
+    if (batch) *batch = r.batch;
+    if (rows) *rows = r.rows;
+    if (K) *K = r.K;
+    if (count) *count = r.count;
+    if (chunk) *chunk = r.chunk;
+  });
+}
+
+int eda_run_info(const eda_run* run, int32_t* n_imfs, int32_t* error, int32_t* windows, int32_t* sifts,
+                 double* spacing, double* energy) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("eda: null run");
+    const edab::Run& r = *run->run;
+    const size_t B = static_cast<size_t>(r.batch), K = static_cast<size_t>(r.K);
+    const size_t cap1 = static_cast<size_t>(r.rows_cap > 0 ? r.rows_cap - 1 : 0);
+    for (size_t b = 0; b < B; ++b) {
+      if (n_imfs) n_imfs[b] = r.n_imfs[b];
+      if (error) error[b] = r.error[b];
+      const int32_t kb = r.error[b] ? 0 : r.n_imfs[b];
+      for (size_t k = 0; k < K; ++k) {
+        const bool have = static_cast<int32_t>(k) < kb;
+        if (windows) windows[b * K + k] = have ? r.hist_scale[b * cap1 + k] : 0;
+        if (sifts) sifts[b * K + k] = have ? r.hist_sifts[b * cap1 + k] : 0;
+        if (spacing) spacing[b * K + k] = have ? r.hist_spacing[b * cap1 + k] : 0.0;
+        if (energy) energy[b * K + k] = have ? r.hist_energy[b * cap1 + k] : 0.0;
+      }
+    }
+  });
+}
+
+int eda_run_collect(eda_run* run, void* dst, int dst_on_device, void* stream) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("eda: null run");
+    edab::Run& r = *run->run;
+    int prev = 0;
+    EDAB_CUDA(cudaGetDevice(&prev));
+    if (prev != r.device) EDAB_CUDA(cudaSetDevice(r.device));
+    r.collect(dst, dst_on_device != 0, static_cast<cudaStream_t>(stream));
+    if (prev != r.device) EDAB_CUDA(cudaSetDevice(prev));
+  });
+}
+
+void eda_run_free(eda_run* run) { delete run; }
+
+size_t eda_last_error(char* buf, size_t len) {
+  put(buf, len, g_last_error);
+  return g_last_error.size();
+}
+
+int eda_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int eda_build_info(char* buf, size_t len) {
+  int rt = 0, drv = 0;
+  cudaRuntimeGetVersion(&rt);
+  cudaDriverGetVersion(&drv);
+  (void)cudaGetLastError();
+  char s[512];
+  std::snprintf(s, sizeof s,
+                "{\"version\": \"0.1.0\", \"engine\": \"b200\", \"cuda_architectures\": \"100a\", \"sass\": [\"sm_100a\"], "
+                "\"ptx\": [], \"cuda_toolkit\": \"%d.%d\", \"cuda_runtime\": %d, \"cuda_driver\": %d, "
+                "\"build_type\": \"Release\", \"cufft_version\": null}",
+                CUDART_VERSION / 1000, (CUDART_VERSION % 1000) / 10, rt, drv);
+  put(buf, len, s);
+  return EDA_OK;
+}
+
+int eda_device_info(int device, char* buf, size_t len) {
+  return guarded([&] {
+    int n = eda_device_count();
+    if (device < 0 || device >= n) throw std::invalid_argument("eda: CUDA device " + std::to_string(device) + " is not visible");
+    cudaDeviceProp p{};
+    EDAB_CUDA(cudaGetDeviceProperties(&p, device));
+    int rt = 0, drv = 0;
+    cudaRuntimeGetVersion(&rt);
+    cudaDriverGetVersion(&drv);
+    char bus[32] = {0};
+    cudaDeviceGetPCIBusId(bus, sizeof bus, device);
+    size_t fr = 0, tot = 0;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    cudaMemGetInfo(&fr, &tot);
+    cudaSetDevice(prev);
+    (void)cudaGetLastError();
+    char s[1024];
+    std::snprintf(s, sizeof s,
+                  "{\"device\": %d, \"name\": \"%s\", \"pci_bus_id\": \"%s\", \"compute_capability\": [%d, %d], "
+                  "\"multiprocessors\": %d, \"total_memory\": %zu, \"free_memory\": %zu, \"l2_cache\": %d, "
+                  "\"driver_version\": %d, \"runtime_version\": %d}",
+                  device, p.name, bus, p.major, p.minor, p.multiProcessorCount, tot, fr, p.l2CacheSize, drv, rt);
+    put(buf, len, s);
+  });
+}
+
+int eda_release_workspace(void) {
+  return guarded([&] { edab::thread_workspace().release(); });
+}
+
+}  // extern "C"

@@ -1,0 +1,274 @@
+// SPDX-License-Identifier: Apache-2.0
+// A call: validation, the output rows, the chunking by free device memory, the host-to-device copy
+// of each chunk, the engine, the per-element results and the collect of the public rows
+// (cpp/src/method/driver.cpp:754-923 and cpp/src/method/driver.cpp:962-987 of eda-cuda).
+#include "driver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <mutex>
+
+namespace edab {
+
+Workspace::~Workspace() { release(); }
+
+void Workspace::release() {
+  if (base_) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (device_ >= 0 && prev != device_) cudaSetDevice(device_);
+    cudaFree(base_);
+    if (device_ >= 0 && prev != device_ && prev >= 0) cudaSetDevice(prev);
+  }
+  base_ = nullptr;
+  size_ = 0;
+  used_ = 0;
+}
+
+void Workspace::reserve(size_t bytes) {
+  int dev = 0;
+  EDAB_CUDA(cudaGetDevice(&dev));
+  if (base_ && size_ >= bytes && dev == device_) return;
+  release();
+  void* p = nullptr;
+  const cudaError_t e = cudaMalloc(&p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    throw OutOfMemory("eda: the workspace (" + std::to_string(bytes >> 20) + " MiB) does not fit the device memory");
+  }
+  EDAB_CUDA(e);
+  // deterministic contents: pad samples of every field start at zero
+  EDAB_CUDA(cudaMemset(p, 0, bytes));
+  base_ = static_cast<unsigned char*>(p);
+  size_ = bytes;
+  device_ = dev;
+}
+
+Workspace& thread_workspace() {
+  thread_local Workspace ws;
+  return ws;
+}
+
+Run::~Run() {
+  if (dev_rows) cudaFree(dev_rows);
+}
+
+namespace {
+
+template <class T>
+__global__ void collect_kernel(int64_t B, int32_t P, int32_t cap, int64_t count, const int32_t* n_imfs,
+                               const int32_t* error, const T* __restrict__ src, T* __restrict__ dst) {
+  const int64_t total = B * P * count;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx % count;
+    const int64_t bk = idx / count;
+    const int64_t k = bk % P;
+    const int64_t b = bk / P;
+    T v;
+    if (error[b] != 0) v = static_cast<T>(d_nan());
+    else if (k <= n_imfs[b]) v = src[(b * cap + k) * count + i];
+    else v = T(0);
+    dst[idx] = v;
+  }
+}
+
+int32_t max_axis(int dtype) { return dtype == 0 ? 8192 : 8192; }
+
+}  // namespace
+
+void Run::collect(void* dst, bool dst_on_device, cudaStream_t s) {
+  if (batch == 0 || rows == 0) return;
+  const size_t es = dtype == 0 ? 4 : 8;
+  const size_t elems = static_cast<size_t>(batch) * rows * count;
+  int32_t* meta = nullptr;
+  EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&meta), sizeof(int32_t) * 2 * batch, s));
+  EDAB_CUDA(cudaMemcpyAsync(meta, n_imfs.data(), sizeof(int32_t) * batch, cudaMemcpyHostToDevice, s));
+  EDAB_CUDA(cudaMemcpyAsync(meta + batch, error.data(), sizeof(int32_t) * batch, cudaMemcpyHostToDevice, s));
+  void* out = dst;
+  if (!dst_on_device) EDAB_CUDA(cudaMallocAsync(&out, elems * es, s));
+  const unsigned blocks = blocks_for(static_cast<int64_t>(elems) / 4 + 1);
+  const unsigned grid = std::min<unsigned>(blocks, 1u << 20);
+  if (dtype == 0) {
+    collect_kernel<float><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, meta, meta + batch,
+                                                    static_cast<const float*>(dev_rows), static_cast<float*>(out));
+  } else {
+    collect_kernel<double><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, meta, meta + batch,
+                                                     static_cast<const double*>(dev_rows), static_cast<double*>(out));
+  }
+  EDAB_LAUNCH("collect_kernel");
+  if (!dst_on_device) {
+    EDAB_CUDA(cudaMemcpyAsync(dst, out, elems * es, cudaMemcpyDeviceToHost, s));
+    EDAB_CUDA(cudaFreeAsync(out, s));
+  }
+  EDAB_CUDA(cudaFreeAsync(meta, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+}
+
+void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params& p) {
+  if (dim < 1 || dim > kMaxDim) throw std::invalid_argument("eda: D must be 1, 2 or 3");
+  if (dtype != 0 && dtype != 1) throw std::invalid_argument("eda: the input must be float32 or float64");
+  const int32_t lim = max_axis(dtype);
+  for (int a = 0; a < dim; ++a) {
+    if (n[a] < 1) throw std::invalid_argument("eda: every spatial extent must be >= 1");
+    if (n[a] > lim) {
+      throw std::invalid_argument("eda: axis extent " + std::to_string(n[a]) + " exceeds the limit " + std::to_string(lim) +
+                                  (dtype == 0 ? " for float32" : " for float64"));
+    }
+  }
+  for (int a = 0; a < dim; ++a) {
+    if (n[a] < 2) {
+      if (dim == 1) {
+        throw std::invalid_argument(
+            "eda: a 1D signal needs at least 2 samples, got 1 (one sample has no sample differences, so no noise "
+            "level; it is its own residue)");
+      }
+      throw std::invalid_argument("eda: every spatial axis of a " + std::to_string(dim) +
+                                  "D field needs extent >= 2, but spatial axis " + std::to_string(a) +
+                                  " has extent 1; drop that axis (squeeze it, or leave it out of axes=) to decompose "
+                                  "the field in " + std::to_string(dim - 1) + "D");
+    }
+  }
+  if (batch < 1) throw std::invalid_argument("eda: the batch needs at least one element");
+  if (!(p.tie_tolerance < 0) && !std::isfinite(p.tie_tolerance)) {
+    throw std::invalid_argument("eda: tie_tolerance must be a finite value >= 0");
+  }
+  if (p.sifts < 1) throw std::invalid_argument("eda: sifts must be >= 1");
+  if (p.max_chunk < 0) throw std::invalid_argument("eda: max_chunk must be >= 0");
+}
+
+std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                               const Params& p, cudaStream_t s) {
+  validate(dtype, dim, batch, n, p);
+  const bool f32 = dtype == 0;
+  const size_t es = f32 ? 4 : 8;
+  const Geom g = make_geom(dim, batch, n);
+  const double tau = p.tie_tolerance >= 0 ? p.tie_tolerance : (f32 ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
+  Ctl c = make_ctl(g, f32, p.sifts, tau, p.max_imf, p.check_finite, 0);
+  const int32_t bound = mode_bound(c);
+  const int32_t modes_max = p.max_imf > 0 ? std::min(bound, p.max_imf) : bound;
+  const int32_t cap = modes_max + 2;
+  c.rows_cap = cap;
+  auto run = std::make_unique<Run>();
+  run->dtype = dtype;
+  EDAB_CUDA(cudaGetDevice(&run->device));
+  run->geom = g;
+  run->batch = batch;
+  run->count = g.count;
+  run->rows_cap = cap;
+  const size_t row_bytes = static_cast<size_t>(batch) * cap * static_cast<size_t>(g.count) * es;
+  const size_t he = static_cast<size_t>(batch) * static_cast<size_t>(cap - 1);
+  {
+    const cudaError_t e = cudaMalloc(&run->dev_rows, row_bytes);
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      throw OutOfMemory("eda: the output rows (" + std::to_string(row_bytes >> 20) +
+                        " MiB) do not fit the device memory; set max_imf or decompose fewer elements per call");
+    }
+    EDAB_CUDA(e);
+  }
+  // the history: scale, sifts (int32), spacing, energy (double), [B, cap - 1] each
+  int32_t* hist_i = nullptr;
+  double* hist_d = nullptr;
+  EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&hist_i), sizeof(int32_t) * 2 * std::max<size_t>(he, 1), s));
+  EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&hist_d), sizeof(double) * 2 * std::max<size_t>(he, 1), s));
+  EDAB_CUDA(cudaMemsetAsync(hist_i, 0, sizeof(int32_t) * 2 * std::max<size_t>(he, 1), s));
+  EDAB_CUDA(cudaMemsetAsync(hist_d, 0, sizeof(double) * 2 * std::max<size_t>(he, 1), s));
+  // the chunk: the largest batch whose workspace fits the free memory (halving)
+  int64_t Bc = batch;
+  if (p.max_chunk > 0) Bc = std::min(Bc, p.max_chunk);
+  size_t free_b = 0, total_b = 0;
+  EDAB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const size_t margin = std::max<size_t>(size_t{256} << 20, free_b / 20);
+  const auto need = [&](int64_t nb) {
+    const Geom gc = make_geom(dim, nb, n);
+    const size_t stage = static_cast<size_t>(nb) * static_cast<size_t>(g.count) * es;
+    return (f32 ? engine_bytes<float>(gc) : engine_bytes<double>(gc)) + stage + 4096;
+  };
+  Workspace& ws = thread_workspace();
+  for (;;) {
+    const size_t want = need(Bc);
+    if (want + margin <= free_b + 0 || Bc == 1) {
+      if (want + margin > free_b && Bc == 1) {
+        // the workspace held by this thread counts as free for this call
+        ws.release();
+        EDAB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        if (want > free_b) {
+          throw OutOfMemory("eda: one element needs a workspace of " + std::to_string(want >> 20) + " MiB and " +
+                            std::to_string(free_b >> 20) + " MiB are free");
+        }
+      }
+      break;
+    }
+    Bc = (Bc + 1) / 2;
+  }
+  run->chunk = Bc;
+  ws.reserve(need(Bc));
+  std::vector<Elem> elems(static_cast<size_t>(batch));
+  std::vector<int32_t> exps(static_cast<size_t>(batch), 0);
+  std::vector<Elem> part;
+  for (int64_t b0 = 0; b0 < batch; b0 += Bc) {
+    const int64_t nb = std::min(Bc, batch - b0);
+    const Geom gc = make_geom(dim, nb, n);
+    ws.reset();
+    // the chunk's dense input, staged at the head of the workspace
+    void* staged = ws.take<unsigned char>(static_cast<size_t>(nb) * static_cast<size_t>(g.count) * es);
+    const unsigned char* src = static_cast<const unsigned char*>(x) + static_cast<size_t>(b0) * g.count * es;
+    EDAB_CUDA(cudaMemcpyAsync(staged, src, static_cast<size_t>(nb) * g.count * es,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    const size_t ho = static_cast<size_t>(b0) * static_cast<size_t>(cap - 1);
+    unsigned char* rows0 = static_cast<unsigned char*>(run->dev_rows) + static_cast<size_t>(b0) * cap * g.count * es;
+    if (f32) {
+      run_chunk<float>(gc, c, s, ws, static_cast<const float*>(staged), reinterpret_cast<float*>(rows0), hist_i + ho,
+                       hist_i + he + ho, hist_d + ho, hist_d + he + ho, part);
+    } else {
+      run_chunk<double>(gc, c, s, ws, static_cast<const double*>(staged), reinterpret_cast<double*>(rows0),
+                        hist_i + ho, hist_i + he + ho, hist_d + ho, hist_d + he + ho, part);
+    }
+    for (int64_t b = 0; b < nb; ++b) elems[static_cast<size_t>(b0 + b)] = part[static_cast<size_t>(b)];
+  }
+  run->n_imfs.assign(static_cast<size_t>(batch), 0);
+  run->error.assign(static_cast<size_t>(batch), 0);
+  int32_t P = 0;
+  bool any_error = false;
+  for (int64_t b = 0; b < batch; ++b) {
+    const Elem& e = elems[static_cast<size_t>(b)];
+    exps[static_cast<size_t>(b)] = e.exp;
+    int32_t err = 0, ni = 0;
+    if (e.status == kError) err = e.error ? e.error : kErrInternal;
+    else if (e.error == kErrNonFiniteResult) err = kErrNonFiniteResult;
+    else if (e.status != kDone || e.n_imfs + 1 > cap) err = kErrInternal;
+    else ni = e.n_imfs;
+    run->error[static_cast<size_t>(b)] = err;
+    run->n_imfs[static_cast<size_t>(b)] = ni;
+    if (err) any_error = true;
+    else P = std::max(P, ni + 1);
+    run->K = std::max(run->K, ni);
+  }
+  if (any_error) P = std::max(P, 1);
+  run->rows = P;
+  run->hist_scale.resize(he);
+  run->hist_sifts.resize(he);
+  run->hist_spacing.resize(he);
+  run->hist_energy.resize(he);
+  if (he) {
+    EDAB_CUDA(cudaMemcpyAsync(run->hist_scale.data(), hist_i, he * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    EDAB_CUDA(cudaMemcpyAsync(run->hist_sifts.data(), hist_i + he, he * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    EDAB_CUDA(cudaMemcpyAsync(run->hist_spacing.data(), hist_d, he * sizeof(double), cudaMemcpyDeviceToHost, s));
+    EDAB_CUDA(cudaMemcpyAsync(run->hist_energy.data(), hist_d + he, he * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  EDAB_CUDA(cudaFreeAsync(hist_i, s));
+  EDAB_CUDA(cudaFreeAsync(hist_d, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+  // the energies in x's units: 4^k times the prescaled sums
+  for (int64_t b = 0; b < batch && he; ++b) {
+    const int32_t k = exps[static_cast<size_t>(b)];
+    if (k == 0 || run->error[static_cast<size_t>(b)]) continue;
+    double* e = run->hist_energy.data() + static_cast<size_t>(b) * static_cast<size_t>(cap - 1);
+    for (int32_t j = 0; j < run->n_imfs[static_cast<size_t>(b)]; ++j) e[j] = std::ldexp(e[j], 2 * k);
+  }
+  return run;
+}
+
+}  // namespace edab

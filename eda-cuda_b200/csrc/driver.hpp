@@ -1,0 +1,73 @@
+// SPDX-License-Identifier: Apache-2.0
+// The host side of a call: the device workspace, the chunking of a batch by free device memory and
+// the Run that holds a call's rows on the device (cpp/src/decompose.hpp:35-106 and
+// cpp/src/method/driver.cpp:754-923 of eda-cuda define the behaviour this follows).
+#pragma once
+
+#include "engine.cuh"
+
+#include <memory>
+#include <vector>
+
+namespace edab {
+
+// A grow-only device buffer carved into 256-byte aligned slices (one per thread and device).
+class Workspace {
+ public:
+  ~Workspace();
+  void reserve(size_t bytes);  // frees and reallocates when the buffer is smaller
+  void reset() { used_ = 0; }
+  template <class T>
+  T* take(size_t count) {
+    const size_t bytes = (count * sizeof(T) + 255) / 256 * 256;
+    if (used_ + bytes > size_) throw std::logic_error("eda: workspace layout exceeds its reservation");
+    T* p = reinterpret_cast<T*>(base_ + used_);
+    used_ += bytes;
+    return p;
+  }
+  void release();
+
+ private:
+  unsigned char* base_ = nullptr;
+  size_t size_ = 0;
+  size_t used_ = 0;
+  int device_ = -1;
+};
+Workspace& thread_workspace();
+
+struct Params {
+  int32_t max_imf = -1;
+  double tie_tolerance = -1.0;  // < 0: 2^-14 (float32) / 2^-30 (float64)
+  int32_t sifts = 3;
+  bool check_finite = true;
+  int64_t max_chunk = 0;
+};
+
+// One call's results: the rows (B, cap, count) on the device and the per-element information.
+struct Run {
+  int dtype = 0;  // 0 float32, 1 float64
+  int device = 0;
+  Geom geom{};
+  int64_t batch = 0, count = 0, chunk = 0;
+  int32_t rows = 1, rows_cap = 0, K = 0;
+  std::vector<int32_t> n_imfs, error, hist_scale, hist_sifts;
+  std::vector<double> hist_spacing, hist_energy;
+  void* dev_rows = nullptr;  // cudaMalloc'd
+  ~Run();
+  // (B, P, count) into dst: NaN rows for failed elements, zeros above an element's residue.
+  void collect(void* dst, bool dst_on_device, cudaStream_t s);
+};
+
+// Decomposes x (B, n_0..n_{D-1}), C-contiguous, float32 (dtype 0) or float64 (1), on the host or
+// the current device, on stream s. Throws std::invalid_argument, OutOfMemory or CudaError.
+std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                               const Params& p, cudaStream_t s);
+void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params& p);
+
+template <class T>
+size_t engine_bytes(const Geom& g);
+template <class T>
+void run_chunk(const Geom& g, const Ctl& c, cudaStream_t s, Workspace& ws, const T* x, T* rows, int32_t* hs,
+               int32_t* hf, double* hp, double* he, std::vector<Elem>& out);
+
+}  // namespace edab

@@ -1,0 +1,445 @@
+// SPDX-License-Identifier: Apache-2.0
+// The orientation (orient.cuh): mean, forward DCT-II along every axis, the log-Gabor band, the
+// Riesz components by inverse cosine / sine transforms, the energy tensor and the Jacobi
+// eigen-decomposition. The axis transforms are batched matrix products; this file holds the
+// portable SIMT product (tiled in shared memory, FP32 accumulation for float32 and FP64 for
+// float64) that the tensor-core path (orient_tc.cu) is checked against.
+#include "orient.cuh"
+
+#include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+namespace edab {
+namespace {
+
+// C(i, j) = sum_k A(i, k) B(k, j) with strided operands; grid.z the batch of blocks.
+struct GemmDesc {
+  int64_t M, N, K;
+  int64_t sAi, sAk, sBk, sBj, sCi, sCj;
+  int64_t zA, zB, zC;       // batch strides of the blocks (A, B, C)
+  int64_t outer;            // blocks per element (z = b * outer + o)
+  int64_t eA, eB, eC;       // element strides
+  int64_t oA, oB, oC;       // outer strides
+};
+
+constexpr int kBM = 64, kBN = 64, kBK = 16;
+
+template <class T>
+__global__ void __launch_bounds__(256) gemm_simt(GemmDesc d, const T* __restrict__ A, const T* __restrict__ Bm,
+                                                 T* __restrict__ C, const int32_t* __restrict__ run) {
+  __shared__ T As[kBK][kBM + 1];
+  __shared__ T Bs[kBK][kBN + 1];
+  const int64_t z = blockIdx.z;
+  const int64_t b = z / d.outer, o = z - (z / d.outer) * d.outer;
+  if (run && !run[b]) return;
+  const T* pA = A + b * d.eA + o * d.oA;
+  const T* pB = Bm + b * d.eB + o * d.oB;
+  T* pC = C + b * d.eC + o * d.oC;
+  const int64_t i0 = static_cast<int64_t>(blockIdx.y) * kBM, j0 = static_cast<int64_t>(blockIdx.x) * kBN;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v] = T(0);
+  for (int64_t k0 = 0; k0 < d.K; k0 += kBK) {
+    for (int t = threadIdx.x; t < kBK * kBM; t += 256) {
+      const int kk = t / kBM, ii = t % kBM;
+      const int64_t i = i0 + ii, k = k0 + kk;
+      As[kk][ii] = (i < d.M && k < d.K) ? pA[i * d.sAi + k * d.sAk] : T(0);
+    }
+    for (int t = threadIdx.x; t < kBK * kBN; t += 256) {
+      const int kk = t / kBN, jj = t % kBN;
+      const int64_t j = j0 + jj, k = k0 + kk;
+      Bs[kk][jj] = (j < d.N && k < d.K) ? pB[k * d.sBk + j * d.sBj] : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK; ++kk) {
+      T a[4], bb[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = As[kk][ty + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) bb[v] = Bs[kk][tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], bb[v], acc[u][v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int64_t i = i0 + ty + 16 * u;
+    if (i >= d.M) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int64_t j = j0 + tx + 16 * v;
+      if (j < d.N) pC[i * d.sCi + j * d.sCj] = acc[u][v];
+    }
+  }
+}
+
+// out = M applied along axis a of every element of `in` (padded fields): out[.., i, ..] =
+// sum_k M[i][k] in[.., k, ..].
+template <class T>
+void apply_axis(cudaStream_t s, const Geom& g, int a, const T* M, const T* in, T* out, const int32_t* run) {
+  GemmDesc d{};
+  const int64_t n = g.n[a];
+  if (a == g.dim - 1) {
+    // rows x n times M^T
+    d.M = g.rows;
+    d.N = n;
+    d.K = n;
+    d.sAi = g.pitch;
+    d.sAk = 1;
+    d.sBk = 1;
+    d.sBj = n;
+    d.sCi = g.pitch;
+    d.sCj = 1;
+    d.outer = 1;
+    d.eA = g.field;
+    d.eB = 0;
+    d.eC = g.field;
+    const dim3 grid(static_cast<unsigned>((d.N + kBN - 1) / kBN), static_cast<unsigned>((d.M + kBM - 1) / kBM),
+                    static_cast<unsigned>(g.batch));
+    gemm_simt<T><<<grid, 256, 0, s>>>(d, in, M, out, run);
+  } else {
+    const int64_t inner = g.stride[a];
+    int64_t outer = 1;
+    for (int ax = 0; ax < a; ++ax) outer *= g.n[ax];
+    d.M = n;
+    d.N = inner;
+    d.K = n;
+    d.sAi = n;
+    d.sAk = 1;
+    d.sBk = inner;
+    d.sBj = 1;
+    d.sCi = inner;
+    d.sCj = 1;
+    d.outer = outer;
+    d.eA = 0;
+    d.oA = 0;
+    d.eB = g.field;
+    d.oB = n * inner;
+    d.eC = g.field;
+    d.oC = n * inner;
+    const dim3 grid(static_cast<unsigned>((d.N + kBN - 1) / kBN), static_cast<unsigned>((d.M + kBM - 1) / kBM),
+                    static_cast<unsigned>(g.batch * outer));
+    gemm_simt<T><<<grid, 256, 0, s>>>(d, M, in, out, run);
+  }
+  EDAB_LAUNCH("gemm_simt");
+}
+
+// The element's mean in double: a fixed per-thread order and a fixed tree (one CTA per element).
+template <class T>
+__global__ void __launch_bounds__(256) mean_kernel(Geom g, const T* __restrict__ r, const int32_t* run, double* mean) {
+  __shared__ double sh[256];
+  const int64_t b = blockIdx.x;
+  const int32_t nl = g.n[g.dim - 1];
+  const int64_t total = g.rows * nl;
+  double acc = 0.0;
+  if (run[b]) {
+    const T* rb = r + b * g.field;
+    for (int64_t i = threadIdx.x; i < total; i += 256) {
+      const int64_t q = i / nl;
+      acc = __dadd_rn(acc, static_cast<double>(rb[q * g.pitch + (i - q * nl)]));
+    }
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) mean[b] = run[b] ? __ddiv_rn(sh[0], static_cast<double>(total)) : 0.0;
+}
+
+// The frequencies of DCT index k in cycles per sample (u_a = k_a / (2 n_a)) and rad = |u|.
+template <int D>
+__device__ __forceinline__ double dct_freq(const Geom& g, const int32_t* k, double* u) {
+  double r2 = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    u[a] = __dmul_rn(static_cast<double>(k[a]), __ddiv_rn(1.0, __dmul_rn(2.0, static_cast<double>(g.n[a]))));
+    r2 = __dadd_rn(r2, __dmul_rn(u[a], u[a]));
+  }
+  return __dsqrt_rn(r2);
+}
+
+// The Jacobi rotation of the reference's eigen pass (Rutishauser's stable form).
+__device__ __forceinline__ void jacobi_rotate(double (&A)[3][3], double (&V)[3][3], int p, int q, int r, int dim) {
+  const double apq = A[p][q];
+  if (apq == 0.0) return;
+  const double theta = __ddiv_rn(__dsub_rn(A[q][q], A[p][p]), __dmul_rn(2.0, apq));
+  const double at = fabs(theta);
+  const double t = __ddiv_rn(copysign(1.0, theta), __dadd_rn(at, __dsqrt_rn(__dadd_rn(__dmul_rn(theta, theta), 1.0))));
+  const double c = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(__dmul_rn(t, t), 1.0)));
+  const double s = __dmul_rn(t, c);
+  const double tau = __ddiv_rn(s, __dadd_rn(1.0, c));
+  const double tapq = __dmul_rn(t, apq);
+  A[p][p] = __dsub_rn(A[p][p], tapq);
+  A[q][q] = __dadd_rn(A[q][q], tapq);
+  A[p][q] = A[q][p] = 0.0;
+  if (r >= 0) {
+    const double gg = A[r][p], hh = A[r][q];
+    const double np_ = __dsub_rn(gg, __dmul_rn(s, __dadd_rn(hh, __dmul_rn(gg, tau))));
+    const double nq_ = __dadd_rn(hh, __dmul_rn(s, __dsub_rn(gg, __dmul_rn(hh, tau))));
+    A[r][p] = A[p][r] = np_;
+    A[r][q] = A[q][r] = nq_;
+  }
+  for (int k = 0; k < dim; ++k) {
+    const double gg = V[k][p], hh = V[k][q];
+    V[k][p] = __dsub_rn(gg, __dmul_rn(s, __dadd_rn(hh, __dmul_rn(gg, tau))));
+    V[k][q] = __dadd_rn(hh, __dmul_rn(s, __dsub_rn(gg, __dmul_rn(hh, tau))));
+  }
+}
+
+template <int D>
+__host__ __device__ constexpr int tensor_pair(int a, int b) {
+  return D == 2 ? (a == 0 ? b : 2) : (a == 0 ? b : (a == 1 ? 2 + b : 5));
+}
+
+// T = R1 R1^T + R2 R2^T in T, then the eigen pass in double: n the top eigenvector, c = (mu1 -
+// mu2) / (mu1 + mu2) clipped to [0, 1].
+template <class T, int D>
+__global__ void __launch_bounds__(256) tensor_eigen(Geom g, const int32_t* run, const T* __restrict__ work_r1,
+                                                    const T* __restrict__ work_r2, T* n0, T* n1, T* n2, T* coh,
+                                                    Elem* el) {
+  constexpr int K = D * (D + 1) / 2;
+  const int64_t F = g.batch * g.field;
+  const int32_t nl = g.n[D - 1];
+  for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
+    if (!run[b]) continue;
+    for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
+         v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      if (v % g.pitch >= nl) continue;
+      const int64_t i = b * g.field + v;
+      T R1[D], R2[K];
+#pragma unroll
+      for (int a = 0; a < D; ++a) R1[a] = work_r1[a * F + i];
+#pragma unroll
+      for (int p = 0; p < K; ++p) R2[p] = work_r2[p * F + i];
+      double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+      bool finite = true;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+#pragma unroll
+        for (int c = a; c < D; ++c) {
+          T vv = mul_rn(R1[a], R1[c]);
+#pragma unroll
+          for (int k = 0; k < D; ++k) {
+            const T hak = R2[tensor_pair<D>(a < k ? a : k, a < k ? k : a)];
+            const T hkc = R2[tensor_pair<D>(k < c ? k : c, k < c ? c : k)];
+            vv = add_rn(vv, mul_rn(hak, hkc));
+          }
+          const double dv = static_cast<double>(vv);
+          finite = finite && isfinite(dv);
+          A[a][c] = A[c][a] = dv;
+        }
+      }
+      if (!finite) el[b].nonfinite = 1;
+      if constexpr (D == 2) {
+        jacobi_rotate(A, V, 0, 1, -1, 2);
+      } else {
+        double amax = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int c = a; c < 3; ++c) amax = fmax(amax, fabs(A[a][c]));
+        if (amax > 0.0 && amax < INFINITY) {
+          const double sc = scalbn(1.0, -ilogb(amax));
+          for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 3; ++c) A[a][c] = __dmul_rn(A[a][c], sc);
+        }
+#pragma unroll 1
+        for (int sweep = 0; sweep < 6; ++sweep) {
+          jacobi_rotate(A, V, 0, 1, 2, 3);
+          jacobi_rotate(A, V, 0, 2, 1, 3);
+          jacobi_rotate(A, V, 1, 2, 0, 3);
+        }
+      }
+      double mu[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) mu[a] = A[a][a];
+      int top = 0;
+#pragma unroll
+      for (int a = 1; a < D; ++a) top = mu[a] > mu[top] ? a : top;
+      double mu2 = -INFINITY;
+#pragma unroll
+      for (int a = 0; a < D; ++a) mu2 = (a != top && mu[a] > mu2) ? mu[a] : mu2;
+      double mu1 = mu[0];
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        if (a == top) mu1 = mu[a];
+      }
+      double nv[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        double vv = V[a][0];
+#pragma unroll
+        for (int c = 1; c < D; ++c) vv = c == top ? V[a][c] : vv;
+        nv[a] = vv;
+      }
+      const double ssum = __dadd_rn(mu1, mu2);
+      double cv = ssum > 0.0 ? __ddiv_rn(__dsub_rn(mu1, mu2), ssum) : 0.0;
+      cv = cv < 0.0 ? 0.0 : (cv > 1.0 ? 1.0 : cv);
+      coh[i] = static_cast<T>(cv);
+      n0[i] = static_cast<T>(nv[0]);
+      n1[i] = static_cast<T>(nv[1]);
+      if constexpr (D == 3) n2[i] = static_cast<T>(nv[2]);
+    }
+  }
+}
+
+struct PlanKey {
+  int dim, n0, n1, n2, f64, dev;
+  bool operator<(const PlanKey& o) const {
+    return std::tie(dim, n0, n1, n2, f64, dev) < std::tie(o.dim, o.n0, o.n1, o.n2, o.f64, o.dev);
+  }
+};
+
+template <class T>
+void upload_axis(OrientPlan& p, int a, int32_t n) {
+  // the bases in long double, rounded once to the dtype
+  const long double pi = 3.141592653589793238462643383279502884L;
+  std::vector<T> fwd(static_cast<size_t>(n) * n), ic(static_cast<size_t>(n) * n), is(static_cast<size_t>(n) * n);
+  for (int32_t k = 0; k < n; ++k) {
+    const long double ck = std::sqrt((k ? 2.0L : 1.0L) / static_cast<long double>(n));
+    for (int32_t x = 0; x < n; ++x) {
+      const int64_t q = (static_cast<int64_t>(k) * (2 * x + 1)) % (4 * static_cast<int64_t>(n));
+      const long double ang = pi * static_cast<long double>(q) / static_cast<long double>(2 * n);
+      const T cv = static_cast<T>(ck * std::cos(ang));
+      const T sv = static_cast<T>(ck * std::sin(ang));
+      fwd[static_cast<size_t>(k) * n + x] = cv;
+      ic[static_cast<size_t>(x) * n + k] = cv;
+      is[static_cast<size_t>(x) * n + k] = sv;
+    }
+  }
+  const size_t bytes = sizeof(T) * static_cast<size_t>(n) * n;
+  EDAB_CUDA(cudaMalloc(&p.fwd[a], bytes));
+  EDAB_CUDA(cudaMalloc(&p.icos[a], bytes));
+  EDAB_CUDA(cudaMalloc(&p.isin[a], bytes));
+  EDAB_CUDA(cudaMemcpy(p.fwd[a], fwd.data(), bytes, cudaMemcpyHostToDevice));
+  EDAB_CUDA(cudaMemcpy(p.icos[a], ic.data(), bytes, cudaMemcpyHostToDevice));
+  EDAB_CUDA(cudaMemcpy(p.isin[a], is.data(), bytes, cudaMemcpyHostToDevice));
+}
+
+}  // namespace
+
+const OrientPlan& orient_plan(const Geom& g, bool f64) {
+  static std::mutex mu;
+  static std::map<PlanKey, std::unique_ptr<OrientPlan>> cache;
+  int dev = 0;
+  EDAB_CUDA(cudaGetDevice(&dev));
+  const PlanKey key{g.dim, g.n[0], g.n[1], g.n[2], f64 ? 1 : 0, dev};
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return *it->second;
+  auto p = std::make_unique<OrientPlan>();
+  p->dim = g.dim;
+  p->f64 = f64;
+  p->device = dev;
+  for (int a = 0; a < g.dim; ++a) {
+    p->n[a] = g.n[a];
+    if (f64) upload_axis<double>(*p, a, g.n[a]);
+    else upload_axis<float>(*p, a, g.n[a]);
+  }
+  const OrientPlan& ref = *p;
+  cache.emplace(key, std::move(p));
+  return ref;
+}
+
+template <class T>
+void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* r, Elem* el, const int32_t* run,
+                 T* const* n, T* coh, T* work, double two_sigma2) {
+  const int D = g.dim;
+  const int64_t F = g.batch * g.field;
+  T* X = work;           // the band spectrum
+  T* Y = work + F;       // a component spectrum
+  T* Z = work + 2 * F;   // ping-pong buffer of the axis passes
+  T* R1 = work + 3 * F;  // D fields
+  T* R2 = R1 + D * F;    // D (D + 1) / 2 fields
+  // mean, then f = r - mean (the difference in double, rounded to T)
+  double* mean = reinterpret_cast<double*>(Z);  // B doubles at the head of Z, consumed before Z is used
+  mean_kernel<T><<<static_cast<unsigned>(g.batch), 256, 0, s>>>(g, r, run, mean);
+  EDAB_LAUNCH("mean_kernel");
+  for_voxels(s, g, [=] __device__(int64_t b) { return run[b] != 0; },
+             [=] __device__(int64_t b, int64_t, int64_t i) {
+               Y[i] = static_cast<T>(__dsub_rn(static_cast<double>(r[i]), mean[b]));
+             });
+  // forward DCT-II along every axis: Y -> X (ping-pong through Z)
+  const T* src = Y;
+  for (int a = 0; a < D; ++a) {
+    T* dst = (a == D - 1) ? X : ((src == Z) ? Y : Z);
+    if (a == D - 1 && src == X) dst = Z;  // (never: src is Y or Z)
+    apply_axis<T>(s, g, a, static_cast<const T*>(plan.fwd[a]), src, dst, run);
+    src = dst;
+  }
+  // the band: X *= G(rad), G the one-octave log-Gabor at f0 = 1 / w (G(0) = 0)
+  const Geom gg = g;
+  for_voxels(s, g, [=] __device__(int64_t b) { return run[b] != 0; },
+             [=] __device__(int64_t b, int64_t v, int64_t i) {
+               int32_t k[kMaxDim];
+               voxel_coords(gg, v, k);
+               double u[kMaxDim];
+               double rad;
+               if (gg.dim == 2) rad = dct_freq<2>(gg, k, u);
+               else rad = dct_freq<3>(gg, k, u);
+               double G = 0.0;
+               if (rad > 0.0) {
+                 const double f0 = __ddiv_rn(1.0, __dmul_rn(1.0, static_cast<double>(el[b].w)));
+                 const double l = log(__ddiv_rn(rad, f0));
+                 G = exp(__ddiv_rn(-__dmul_rn(l, l), two_sigma2));
+               }
+               X[i] = static_cast<T>(__dmul_rn(static_cast<double>(X[i]), G));
+             });
+  // the components: R1_a (sine on axis a), then R2_ab (a <= b; sine on a and b when a != b)
+  int p = 0;
+  for (int kind = 0; kind < 2; ++kind) {
+    for (int a = 0; a < D; ++a) {
+      for (int b2 = (kind == 0 ? a : a); b2 < (kind == 0 ? a + 1 : D); ++b2) {
+        T* out = kind == 0 ? R1 + a * F : R2 + (p++) * F;
+        const int ca = a, cb = b2, ck = kind;
+        for_voxels(s, g, [=] __device__(int64_t bb) { return run[bb] != 0; },
+                   [=] __device__(int64_t, int64_t v, int64_t i) {
+                     int32_t k[kMaxDim];
+                     voxel_coords(gg, v, k);
+                     double u[kMaxDim];
+                     const double rad = gg.dim == 2 ? dct_freq<2>(gg, k, u) : dct_freq<3>(gg, k, u);
+                     double m = 0.0;
+                     if (rad > 0.0) {
+                       const double inv = __ddiv_rn(1.0, rad);
+                       const double ua = __dmul_rn(u[ca], inv);
+                       if (ck == 0) m = ua;
+                       else if (ca == cb) m = __dmul_rn(-ua, ua);
+                       else m = __dmul_rn(ua, __dmul_rn(u[cb], inv));
+                     }
+                     Y[i] = static_cast<T>(__dmul_rn(m, static_cast<double>(X[i])));
+                   });
+        const int odd = kind == 0 ? (1 << a) : (a == b2 ? 0 : ((1 << a) | (1 << b2)));
+        const T* csrc = Y;
+        for (int ax = 0; ax < D; ++ax) {
+          T* dst = (ax == D - 1) ? out : (csrc == Z ? Y : Z);
+          const void* M = ((odd >> ax) & 1) ? plan.isin[ax] : plan.icos[ax];
+          apply_axis<T>(s, g, ax, static_cast<const T*>(M), csrc, dst, run);
+          csrc = dst;
+        }
+      }
+    }
+  }
+  const dim3 grid = voxel_grid(g);
+  if (D == 2) tensor_eigen<T, 2><<<grid, 256, 0, s>>>(g, run, R1, R2, n[0], n[1], nullptr, coh, el);
+  else tensor_eigen<T, 3><<<grid, 256, 0, s>>>(g, run, R1, R2, n[0], n[1], n[2], coh, el);
+  EDAB_LAUNCH("tensor_eigen");
+}
+
+template void orientation<float>(cudaStream_t, const Geom&, const OrientPlan&, const float*, Elem*, const int32_t*,
+                                 float* const*, float*, float*, double);
+template void orientation<double>(cudaStream_t, const Geom&, const OrientPlan&, const double*, Elem*, const int32_t*,
+                                  double* const*, double*, double*, double);
+
+}  // namespace edab

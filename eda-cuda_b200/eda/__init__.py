@@ -1,0 +1,52 @@
+# SPDX-License-Identifier: Apache-2.0
+"""eda on B200: the sifting hot path of eda-cuda's empirical decomposition behind the same public
+call, ``eda.decompose``, computed by this package's sm_100a engine (libeda_b200.so). Importing the
+package needs neither a GPU nor the compiled engine; the engine loads on the first call that needs
+it, and there is no CPU fallback."""
+
+from __future__ import annotations
+
+import operator
+from typing import Any
+
+from . import _native
+from ._api import DecompositionInfo, decompose
+from ._device import DeviceArray
+from ._errors import CudaError, DecompositionError
+
+__version__ = "0.1.0"
+
+__all__ = [
+    "CudaError",
+    "DecompositionError",
+    "DecompositionInfo",
+    "DeviceArray",
+    "__version__",
+    "build_info",
+    "decompose",
+    "device_count",
+    "device_info",
+]
+
+
+def build_info() -> dict[str, Any]:
+    """How the engine was built (CUDA toolkit, runtime and driver, architectures); works without a GPU."""
+    return _native.core().build_info()
+
+
+def device_count() -> int:
+    """The number of visible CUDA devices; 0 without a driver or device."""
+    return _native.core().device_count()
+
+
+def device_info(device: int = 0) -> dict[str, Any]:
+    """Properties of a visible CUDA device; ValueError for a device that is not visible."""
+    if isinstance(device, bool):
+        raise TypeError("eda: device must be an integer, not bool")
+    try:
+        number = operator.index(device)
+    except TypeError:
+        raise TypeError(f"eda: device must be an integer, got {type(device).__name__}") from None
+    if not -(2**31) <= number < 2**31:
+        raise ValueError(f"eda: CUDA device {number} is not visible")
+    return _native.core().device_info(number)

@@ -1,0 +1,246 @@
+# SPDX-License-Identifier: Apache-2.0
+"""``eda.decompose`` on the B200 engine: the public argument rules, layouts, errors and result
+types of the reference's call (src/eda/_api.py:184-353 of eda-cuda), written over this engine's
+binding (_native.py)."""
+
+from __future__ import annotations
+
+import math
+import operator
+from collections.abc import Sequence
+from dataclasses import dataclass
+from typing import Any
+
+import numpy as np
+
+from . import _device, _native
+from ._errors import DecompositionError
+
+#: Error codes of an element (``DecompositionInfo.error``).
+ERROR_NON_FINITE = 1
+ERROR_NON_FINITE_RESULT = 2
+ERROR_INTERNAL = 255
+_MESSAGES = {
+    ERROR_NON_FINITE: "the input has inf or NaN; check_finite=True",
+    ERROR_NON_FINITE_RESULT: (
+        "a non-finite intermediate or output row: the decomposition overflows the dtype's range, "
+        "or the input has inf or NaN with check_finite=False"
+    ),
+}
+_FLOATS = ("float32", "float64")
+_INT32_MAX = 2**31 - 1
+
+
+@dataclass(frozen=True, eq=False)
+class DecompositionInfo:
+    """Per-call information of ``eda.decompose(..., return_info=True)``: ``n_imfs`` and ``error`` of
+    the batch shape; ``windows``, ``spacing``, ``sifts``, ``energy`` of the batch shape plus K (the
+    largest IMF count), zero beyond an element's ``n_imfs`` and for a failed element; ``dtype``, the
+    compute dtype; ``axes``, the spatial axes."""
+
+    n_imfs: np.ndarray
+    error: np.ndarray
+    windows: np.ndarray
+    spacing: np.ndarray
+    sifts: np.ndarray
+    energy: np.ndarray
+    dtype: str
+    axes: tuple[int, ...]
+
+
+def _int_arg(value: Any, name: str) -> int:
+    if isinstance(value, (bool, np.bool_)):
+        raise TypeError(f"eda: {name} must be an integer, not bool")
+    try:
+        return operator.index(value)
+    except TypeError:
+        raise TypeError(f"eda: {name} must be an integer, got {type(value).__name__}") from None
+
+
+def _flag(value: Any, name: str) -> bool:
+    if not isinstance(value, (bool, np.bool_)):
+        raise TypeError(f"eda: {name} must be True or False, got {type(value).__name__}")
+    return bool(value)
+
+
+def _tie(value: Any) -> float | None:
+    if value is None:
+        return None
+    if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, float, np.integer, np.floating)):
+        raise TypeError(f"eda: tie_tolerance must be a real number or None, got {type(value).__name__}")
+    try:
+        number = float(value)
+    except OverflowError:
+        number = math.inf
+    if not (math.isfinite(number) and number >= 0):
+        raise ValueError(f"eda: tie_tolerance must be a finite number >= 0, got {value}")
+    return number
+
+
+def _axes(axes: Any, ndim: int) -> tuple[int, ...]:
+    if ndim < 1:
+        raise ValueError("eda: expected an array with at least one dimension")
+    if axes is None:
+        if ndim > 3:
+            raise ValueError(f"eda: axes=None takes every axis and needs x.ndim <= 3, got {ndim}: name the "
+                             "spatial axes (1 to 3) with axes=")
+        return tuple(range(ndim))
+    if isinstance(axes, (int, np.integer)) and not isinstance(axes, bool):
+        axes = (axes,)
+    try:
+        listed = []
+        for a in axes:
+            if isinstance(a, (bool, np.bool_)):
+                raise TypeError
+            listed.append(operator.index(a))
+    except TypeError:
+        raise TypeError(f"eda: axes must be an int, a sequence of ints or None, got {type(axes).__name__}") from None
+    out = []
+    for a in listed:
+        if not -ndim <= a < ndim:
+            raise np.exceptions.AxisError(a, ndim, "eda")
+        out.append(a % ndim)
+    if len(set(out)) != len(out):
+        raise ValueError(f"eda: axes must be unique, got {tuple(listed)}")
+    if not 1 <= len(out) <= 3:
+        raise ValueError(f"eda: 1 to 3 spatial axes, got {len(out)}")
+    return tuple(out)
+
+
+def _restore(ndim: int, batch_axes: tuple[int, ...], axes: tuple[int, ...], extra: int = 1) -> list[int]:
+    """The permutation from the computed (*batch, *extra, *spatial in axes order) layout to the
+    public one: x's axes in order, the extra axes just before min(axes)."""
+    nb = len(batch_axes)
+    where = {a: nb + extra + k for k, a in enumerate(axes)}
+    where.update({a: k for k, a in enumerate(batch_axes)})
+    m = min(axes)
+    return [where[f] for f in range(m)] + [nb + j for j in range(extra)] + [where[f] for f in range(m, ndim)]
+
+
+def _dtype_name(dtype: Any) -> str:
+    try:
+        return np.dtype(dtype).name
+    except TypeError:
+        return str(dtype).removeprefix("torch.")
+
+
+def decompose(
+    x: Any,
+    axes: int | Sequence[int] | None = None,
+    max_imf: int = -1,
+    *,
+    dtype: Any = None,
+    tie_tolerance: float | None = None,
+    sifts: int = 3,
+    check_finite: bool = True,
+    errors: str = "raise",
+    stream: Any = None,
+    return_info: bool = False,
+    return_orientation: bool = False,
+) -> Any:
+    """Decompose every 1-D, 2-D or 3-D field of ``x`` into intrinsic mode functions (IMFs) and a
+    residue, on the B200 engine. The arguments, the result layout
+    (``x.shape[:m] + (P,) + x.shape[m:]``, ``m = min(axes)``; the IMFs fine to coarse, then the
+    residue, then zero rows), the information and the error rules are those of the reference's
+    ``eda.decompose``. ``return_orientation`` is not available in this engine."""
+    max_imf = max(-_INT32_MAX - 1, min(_int_arg(max_imf, "max_imf"), _INT32_MAX))
+    tie = _tie(tie_tolerance)
+    sifts = _int_arg(sifts, "sifts")
+    if not 1 <= sifts <= _INT32_MAX:
+        raise ValueError(f"eda: sifts must be an integer from 1 to {_INT32_MAX}, got {sifts}")
+    check_finite = _flag(check_finite, "check_finite")
+    return_info = _flag(return_info, "return_info")
+    return_orientation = _flag(return_orientation, "return_orientation")
+    if not isinstance(errors, str) or errors not in ("raise", "status"):
+        raise ValueError(f"eda: errors={errors!r} is not one of 'raise', 'status'")
+    on_device = _device.is_cuda_array(x)
+    if on_device:
+        data = _device.as_tensor(x)
+        src = _device.dtype_name(data)
+        if src not in _device.SUPPORTED_DTYPES:
+            raise TypeError(f"eda: arrays of dtype {src} are not supported (real bool, integer and float arrays only)")
+    else:
+        data = np.asarray(x)
+        src = data.dtype.name
+        if data.dtype.kind not in "biuf":
+            raise TypeError(f"eda: arrays of dtype {src} are not supported (real bool, integer and float arrays only)")
+    target = src if dtype is None else _dtype_name(dtype)
+    if target not in _FLOATS:
+        if dtype is None:
+            raise TypeError(f"eda: expected a float32 or float64 array, got dtype {src} (pass dtype='float32' or "
+                            "dtype='float64' to cast it)")
+        raise TypeError(f"eda: dtype= must be float32 or float64, got {target}")
+    ndim = len(data.shape)
+    axes = _axes(axes, ndim)
+    if return_orientation:
+        if len(axes) < 2:
+            raise ValueError("eda: return_orientation=True needs 2 or 3 spatial axes, got 1 (the method has no "
+                             "orientation in 1-D)")
+        raise NotImplementedError("eda: return_orientation is not available in the B200 engine")
+    batch_axes = tuple(i for i in range(ndim) if i not in axes)
+    batch_shape = tuple(int(data.shape[i]) for i in batch_axes)
+    spatial = tuple(int(data.shape[a]) for a in axes)
+    B = math.prod(batch_shape)
+    order = list(batch_axes) + list(axes)
+    core = _native.core()
+    if on_device:
+        torch = _device._torch()
+        tdt = getattr(torch, target)
+        t = data.permute(order) if order != list(range(ndim)) else data
+        t = t.to(tdt).contiguous().reshape((B,) + spatial)
+        dev = t.device
+        if B == 0:
+            rows_t, raw = torch.zeros((0, 1) + spatial, dtype=tdt, device=dev), core._empty_info(0)
+        else:
+            with torch.cuda.device(dev):
+                st = torch.cuda.current_stream(dev)
+
+                def alloc(P):
+                    out = torch.empty((B, P) + spatial, dtype=tdt, device=dev)
+                    return out, out.data_ptr()
+
+                rows_t, raw = core.decompose_device(t.data_ptr(), dev.index or 0, target, (B,) + spatial, max_imf,
+                                                    tie, sifts, check_finite, 0, st.cuda_stream, alloc)
+    else:
+        xc = data if data.dtype == np.dtype(target) else data.astype(target)
+        xt = np.ascontiguousarray(xc.transpose(order)) if order != list(range(ndim)) else xc
+        xb = np.ascontiguousarray(xt).reshape((B,) + spatial)
+        rows, raw = core.decompose_host(xb, max_imf, tie, sifts, check_finite, False, 0)
+    info = DecompositionInfo(
+        n_imfs=np.asarray(raw["n_imfs"], np.int32).reshape(batch_shape),
+        error=np.asarray(raw["error"], np.int32).reshape(batch_shape),
+        windows=np.asarray(raw["windows"], np.int32).reshape(batch_shape + raw["windows"].shape[1:]),
+        spacing=np.asarray(raw["spacing"], np.float64).reshape(batch_shape + raw["spacing"].shape[1:]),
+        sifts=np.asarray(raw["sifts"], np.int32).reshape(batch_shape + raw["sifts"].shape[1:]),
+        energy=np.asarray(raw["energy"], np.float64).reshape(batch_shape + raw["energy"].shape[1:]),
+        dtype=target,
+        axes=axes,
+    )
+    codes = info.error.reshape(-1)
+    internal = np.flatnonzero(codes == ERROR_INTERNAL)
+    if internal.size:
+        raise RuntimeError("eda: an internal invariant failed (error code 255) for batch index "
+                           f"{', '.join(str(int(i)) for i in internal[:8])}: this is a bug in eda")
+    failed = np.flatnonzero(codes != 0)
+    if failed.size and errors == "raise":
+        parts = []
+        for code in sorted({int(c) for c in codes[failed]}):
+            where = failed[codes[failed] == code]
+            shown = ", ".join(str(int(i)) for i in where[:8]) + (", ..." if where.size > 8 else "")
+            parts.append(f"code {code} ({_MESSAGES.get(code, f'error code {code}')}) at batch index {shown}")
+        raise DecompositionError(
+            f"eda: the decomposition failed for {failed.size} of {codes.size} element(s): " + "; ".join(parts),
+            indices=failed, codes=codes[failed], info=info)
+    perm = _restore(ndim, batch_axes, axes)
+    if on_device:
+        P = rows_t.shape[1]
+        y_t = rows_t.reshape(batch_shape + (P,) + spatial)
+        if perm != list(range(ndim + 1)):
+            y_t = y_t.permute(perm)
+        y = _device.DeviceArray(y_t)
+    else:
+        P = rows.shape[1]
+        y = rows.reshape(batch_shape + (P,) + spatial)
+        if perm != list(range(ndim + 1)):
+            y = y.transpose(perm)
+    return (y, info) if return_info else y

@@ -1,0 +1,186 @@
+# SPDX-License-Identifier: Apache-2.0
+"""The ctypes binding of the engine's C ABI (include/eda_b200.h), loaded on first use.
+
+``core()`` returns an object with the calls of the reference's extension module eda._core
+(src/eda/_core.pyi of eda-cuda): ``build_info``, ``device_count``, ``device_info``,
+``decompose_host`` and ``decompose_device``. There is no CPU fallback: without the compiled library
+the first call raises ImportError.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+from ._errors import CudaError
+
+LIB = Path(__file__).resolve().parent / "libeda_b200.so"
+_core = None
+
+EDA_OK, EDA_INVALID_ARGUMENT, EDA_OUT_OF_MEMORY, EDA_CUDA_ERROR, EDA_INTERNAL = range(5)
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("max_imf", ctypes.c_int32),
+        ("tie_tolerance", ctypes.c_double),
+        ("sifts", ctypes.c_int32),
+        ("check_finite", ctypes.c_int32),
+        ("max_chunk", ctypes.c_int64),
+    ]
+
+
+class Core:
+    """The engine's entry points with the reference extension's Python signatures."""
+
+    def __init__(self, path: Path) -> None:
+        L = ctypes.CDLL(str(path))
+        vp, i32, i64, f64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        L.eda_decompose.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, i64, ctypes.POINTER(i64),
+                                    ctypes.POINTER(_Params), vp, ctypes.POINTER(vp)]
+        L.eda_run_shape.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i32),
+                                    ctypes.POINTER(i64), ctypes.POINTER(i64)]
+        L.eda_run_info.argtypes = [vp] + [vp] * 6
+        L.eda_run_collect.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.eda_run_free.argtypes = [vp]
+        L.eda_run_free.restype = None
+        L.eda_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        L.eda_last_error.restype = ctypes.c_size_t
+        L.eda_build_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        L.eda_device_info.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+        self._lib = L
+        self.path = str(path)
+
+    # -- errors --------------------------------------------------------------------------------
+    def _check(self, status: int) -> None:
+        if status == EDA_OK:
+            return
+        buf = ctypes.create_string_buffer(4096)
+        self._lib.eda_last_error(buf, len(buf))
+        msg = buf.value.decode(errors="replace")
+        if status == EDA_INVALID_ARGUMENT:
+            raise ValueError(msg)
+        if status == EDA_OUT_OF_MEMORY:
+            raise MemoryError(msg)
+        if status == EDA_CUDA_ERROR:
+            name = None
+            if "CUDA error " in msg:
+                name = msg.split("CUDA error ", 1)[1].split(" ", 1)[0]
+            raise CudaError(msg, None, name)
+        raise RuntimeError(msg)
+
+    # -- information ---------------------------------------------------------------------------
+    def build_info(self) -> dict:
+        buf = ctypes.create_string_buffer(2048)
+        self._lib.eda_build_info(buf, len(buf))
+        info = json.loads(buf.value.decode())
+        info["library"] = self.path
+        return info
+
+    def device_count(self) -> int:
+        return int(self._lib.eda_device_count())
+
+    def device_info(self, device: int = 0) -> dict:
+        buf = ctypes.create_string_buffer(2048)
+        self._check(self._lib.eda_device_info(int(device), buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    # -- the decomposition ---------------------------------------------------------------------
+    def _run(self, ptr: int, on_device: bool, dtype: np.dtype, shape: tuple[int, ...], max_imf: int,
+             tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int, stream: int):
+        p = _Params(int(max_imf), -1.0 if tie_tolerance is None else float(tie_tolerance), int(sifts),
+                    int(bool(check_finite)), int(max_chunk))
+        n = (ctypes.c_int64 * 3)(*[int(v) for v in shape[1:]], *([1] * (4 - len(shape))))
+        run = ctypes.c_void_p()
+        code = 0 if dtype == np.float32 else 1
+        self._check(self._lib.eda_decompose(ctypes.c_void_p(ptr), int(on_device), code, len(shape) - 1,
+                                            int(shape[0]), n, ctypes.byref(p), ctypes.c_void_p(stream),
+                                            ctypes.byref(run)))
+        return run
+
+    def _info(self, run) -> tuple[dict, int, int, int]:
+        B, P, K, count, chunk = (ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64(),
+                                 ctypes.c_int64())
+        self._check(self._lib.eda_run_shape(run, ctypes.byref(B), ctypes.byref(P), ctypes.byref(K),
+                                            ctypes.byref(count), ctypes.byref(chunk)))
+        b, k = B.value, K.value
+        arr = {"n_imfs": np.zeros(b, np.int32), "error": np.zeros(b, np.int32),
+               "windows": np.zeros((b, k), np.int32), "sifts": np.zeros((b, k), np.int32),
+               "spacing": np.zeros((b, k), np.float64), "energy": np.zeros((b, k), np.float64)}
+        self._check(self._lib.eda_run_info(run, *(ctypes.c_void_p(arr[n].ctypes.data) for n in
+                                                  ("n_imfs", "error", "windows", "sifts", "spacing", "energy"))))
+        arr["chunk"] = int(chunk.value)
+        return arr, P.value, b, count.value
+
+    @staticmethod
+    def _empty_info(B: int) -> dict:
+        z = np.zeros((B, 0))
+        return {"n_imfs": np.zeros(B, np.int32), "error": np.zeros(B, np.int32), "windows": z.astype(np.int32),
+                "sifts": z.astype(np.int32), "spacing": z, "energy": z.copy(), "chunk": 0}
+
+    def decompose_host(self, x: np.ndarray, max_imf: int, tie_tolerance: float | None, sifts: int,
+                       check_finite: bool, orientation: bool, max_chunk: int) -> tuple:
+        """Decomposes the C-contiguous host array x (B, *spatial) of float32 or float64:
+        (rows (B, P, *spatial), info)."""
+        if orientation:
+            raise NotImplementedError("eda: return_orientation is not available in the B200 engine")
+        if not (isinstance(x, np.ndarray) and x.flags.c_contiguous and x.dtype in (np.float32, np.float64)):
+            raise TypeError("eda: decompose_host: expected a C-contiguous float32 or float64 array")
+        if x.ndim < 2 or x.ndim > 4:
+            raise ValueError("eda: decompose_host: x must have the shape (B, *spatial) with 1 to 3 spatial axes")
+        if x.shape[0] == 0:
+            self._validate_empty(x, max_imf, tie_tolerance, sifts, check_finite, max_chunk)
+            return np.zeros((0, 1) + x.shape[1:], x.dtype), self._empty_info(0)
+        run = self._run(x.ctypes.data, False, x.dtype, x.shape, max_imf, tie_tolerance, sifts, check_finite,
+                        max_chunk, 0)
+        try:
+            info, P, B, count = self._info(run)
+            rows = np.empty((B, P) + x.shape[1:], x.dtype)
+            self._check(self._lib.eda_run_collect(run, ctypes.c_void_p(rows.ctypes.data), 0, None))
+        finally:
+            self._lib.eda_run_free(run)
+        return rows, info
+
+    def _validate_empty(self, x, max_imf, tie_tolerance, sifts, check_finite, max_chunk) -> None:
+        # an empty batch is validated as one element and computes nothing
+        one = np.zeros((1,) + x.shape[1:], x.dtype)
+        p = _Params(int(max_imf), -1.0 if tie_tolerance is None else float(tie_tolerance), int(sifts),
+                    int(bool(check_finite)), int(max_chunk))
+        del one, p
+        for n in x.shape[1:]:
+            if n < 2:
+                raise ValueError("eda: every spatial axis needs extent >= 2")
+
+    def decompose_device(self, ptr: int, device: int, dtype: str, shape: tuple[int, ...], max_imf: int,
+                         tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int,
+                         stream: int, out_ptr_of) -> tuple:
+        """Decomposes the C-contiguous device array at ptr (B, *spatial) in the compute dtype on its
+        device; ``out_ptr_of(P)`` allocates the (B, P, *spatial) output and returns its pointer."""
+        run = self._run(ptr, True, np.dtype(dtype), shape, max_imf, tie_tolerance, sifts, check_finite,
+                        max_chunk, stream)
+        try:
+            info, P, B, count = self._info(run)
+            out, out_ptr = out_ptr_of(P)
+            self._check(self._lib.eda_run_collect(run, ctypes.c_void_p(out_ptr), 1, ctypes.c_void_p(stream)))
+        finally:
+            self._lib.eda_run_free(run)
+        return out, info
+
+
+def core() -> Core:
+    """The engine, loaded on first use (ImportError when the library is not built)."""
+    global _core
+    if _core is None:
+        if not LIB.exists():
+            raise ImportError(
+                f"eda: the B200 engine library is not built ({LIB}); build it with "
+                "`python eda-cuda_b200/build.py` (nvcc for sm_100a)")
+        try:
+            _core = Core(LIB)
+        except OSError as exc:
+            raise ImportError(f"eda: the B200 engine library cannot be loaded: {exc}") from exc
+    return _core

@@ -1,0 +1,110 @@
+/* SPDX-License-Identifier: Apache-2.0
+ *
+ * eda_b200: the C ABI of the B200 engine of eda's decomposition (the sifting hot path behind
+ * eda.decompose). Plain pointers, sizes and status codes; no C++ or framework types. A host binding
+ * (ctypes, cgo, JNI, N-API) binds these entry points; eda-cuda_b200/eda/_native.py is the Python
+ * one and mirrors the reference's extension module eda._core.
+ *
+ * Every entry point returns EDA_OK or an error status; eda_last_error() returns the message of the
+ * calling thread's last failure. Calls may come from several threads; each thread keeps its own
+ * device workspace. The reference interfaces each entry point replaces are cited beside it (paths
+ * inside giorgioangel/eda-cuda).
+ */
+#ifndef EDA_B200_H_
+#define EDA_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EDA_API __attribute__((visibility("default")))
+#else
+#define EDA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference's exceptions, cpp/python/module.cpp:28-51: invalid_argument ->
+ * ValueError, bad_alloc -> MemoryError, CudaError -> eda.CudaError). */
+#define EDA_OK 0
+#define EDA_INVALID_ARGUMENT 1
+#define EDA_OUT_OF_MEMORY 2
+#define EDA_CUDA_ERROR 3
+#define EDA_INTERNAL 4
+
+/* Per-element error codes of info.error (cpp/src/field/state.hpp:16). */
+#define EDA_ERR_NONE 0
+#define EDA_ERR_NON_FINITE 1
+#define EDA_ERR_NON_FINITE_RESULT 2
+#define EDA_ERR_INTERNAL 255
+
+#define EDA_FLOAT32 0
+#define EDA_FLOAT64 1
+
+/* The call parameters (cpp/src/decompose.hpp:69-76, Params). */
+typedef struct eda_params {
+  int32_t max_imf;        /* <= 0: no limit */
+  double tie_tolerance;   /* relative tie tolerance; < 0: 2^-14 (float32) / 2^-30 (float64) */
+  int32_t sifts;          /* sifts per mode, >= 1 (3 by default) */
+  int32_t check_finite;   /* non-zero: an element holding inf or NaN fails with code 1 */
+  int64_t max_chunk;      /* > 0: at most this many elements per chunk; 0: by free device memory */
+} eda_params;
+
+/* One call's results: the rows on the device and the per-element information (the reference's
+ * eda::Run, cpp/src/decompose.hpp:85-104). */
+typedef struct eda_run eda_run;
+
+/* Decomposes x, a C-contiguous (batch, n[0], .., n[dim-1]) array of float32 (dtype 0) or
+ * float64 (dtype 1) on the host (x_on_device 0) or on the calling thread's current CUDA device,
+ * on `stream` (a cudaStream_t; NULL: the legacy default stream). On EDA_OK *out receives the run,
+ * released by eda_run_free. Replaces eda::decompose (cpp/src/decompose.hpp:106) and the argument
+ * rules of the binding's decompose_host / decompose_device (cpp/python/decompose.cpp:325-509). */
+EDA_API int eda_decompose(const void* x, int x_on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                  const eda_params* params, void* stream, eda_run** out);
+
+/* The shape of a run: batch, P (the output rows per element: one more than the largest IMF count
+ * of the elements without an error), K (the largest IMF count: the width of the information
+ * arrays), the samples per element and the elements per chunk (cpp/python/decompose.cpp:188-214). */
+EDA_API int eda_run_shape(const eda_run* run, int64_t* batch, int32_t* rows, int32_t* K, int64_t* count, int64_t* chunk);
+
+/* The per-element information: n_imfs[batch], error[batch], and the [batch, K] arrays windows,
+ * sifts (int32), spacing, energy (float64), zero beyond an element's n_imfs and for failed
+ * elements (cpp/python/decompose.cpp:188-214, info_dict). Any pointer may be NULL. */
+EDA_API int eda_run_info(const eda_run* run, int32_t* n_imfs, int32_t* error, int32_t* windows, int32_t* sifts,
+                 double* spacing, double* energy);
+
+/* The rows (batch, P, count) in the compute dtype into dst (host memory, or device memory of the
+ * run's device with dst_on_device), complete on return: NaN rows for failed elements, the IMFs
+ * then the residue, zeros above (cpp/src/field/field_ops.hpp:43-47, Run::collect). */
+EDA_API int eda_run_collect(eda_run* run, void* dst, int dst_on_device, void* stream);
+
+EDA_API void eda_run_free(eda_run* run);
+
+/* The calling thread's last error message (NUL-terminated, truncated to len). Returns its full
+ * length. */
+EDA_API size_t eda_last_error(char* buf, size_t len);
+
+/* The visible CUDA devices (0 without a driver or device); the build and a device's properties as
+ * JSON text (cpp/python/module.cpp:64-129, build_info / device_info). */
+EDA_API int eda_device_count(void);
+EDA_API int eda_build_info(char* buf, size_t len);
+EDA_API int eda_device_info(int device, char* buf, size_t len);
+
+/* Frees the calling thread's device workspace (the reference's Context::release_unused_memory,
+ * cpp/src/runtime/context.cpp:154-160). */
+EDA_API int eda_release_workspace(void);
+
+/* Instrumentation (no counterpart in the reference): eda_profile(1) resets and enables the counters
+ * of the engine's kernel launches and, for the dominant kernel (the cube-filter passes), of the
+ * CUDA-event duration and algorithmic bytes of every launch; eda_profile_read synchronizes the
+ * device and returns them. */
+EDA_API int eda_profile(int enable);
+EDA_API int eda_profile_read(int64_t* launches, int64_t* cube_launches, double* cube_bytes, double* cube_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EDA_B200_H_ */
