@@ -12,13 +12,15 @@
 // Box sums run axis 0 first and the last pass multiplies by fl_T(1 / prod of the clamped sides);
 // max and min fold the integer order keys of the values (the order of max_c / min_c).
 //
-// B200 design. A CTA stages P whole lines of one element in shared memory (one padding word per
-// 32 samples, so chunk walks 32 samples apart hit distinct banks): rows of the contiguous axis
-// with coalesced loads, or a panel of P adjacent columns of an outer axis (P samples per row
-// segment: whole 32-byte sectors). Work is a flat list of fold tasks, one thread per (line,
-// direction, segment, chunk): chunk totals, the per-segment carries, then H and G folds that
-// replace the staged output in place. The first pass of a cube stages its input once and runs
-// every rung of the ladder on it (the operators' rung group), the later passes one CTA per rung.
+// B200 design. A CTA stages P lines of one element (rows of the contiguous axis, or a panel of P
+// adjacent columns of an outer axis: whole 32-byte sectors) in shared memory, interleaved: sample i
+// of line p at i * PP + p. Lanes map to lines: P lanes of a warp ("a worker") run the same fold
+// task on their P lines, so control flow is uniform and a worker's shared-memory accesses are
+// consecutive words. The fold tasks (one per direction, segment and 32-sample chunk) are spread over
+// the CTA's workers: chunk totals, per-segment exclusive carries, then the H folds and the G folds
+// combined with them; reflection is evaluated only in the chunks that cross a line end. The first
+// pass of a cube stages its input once and runs every rung of the ladder on it (the operators'
+// rung group); later passes run one rung per CTA.
 #include "engine.cuh"
 
 #include <algorithm>
@@ -28,10 +30,12 @@ namespace edab {
 namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
+constexpr int kWarps = kThreads / 32;
 
-__device__ __forceinline__ int32_t pidx(int32_t i) { return i + (i >> 5); }
-__host__ __device__ inline int32_t line_slots(int32_t n) { return n + ((n + 31) >> 5) + 1; }
-__host__ __device__ inline int32_t tot_slots(int32_t n) { return n / 4 + 40; }
+__host__ __device__ inline int32_t tot_slots(int32_t n) { return n / 8 + 24; }
+// Words per staged sample row: P lines plus one (odd, so a transposed row staging of 32
+// consecutive samples hits 32 distinct banks); one line is stored contiguously.
+__host__ __device__ inline int32_t line_pitch(int P) { return P == 1 ? 1 : P + 1; }
 
 // Order key of v as a T-sized integer (its own inverse): integer order = order of max_c/min_c.
 __device__ __forceinline__ float okey(float v) {
@@ -77,96 +81,124 @@ __device__ __forceinline__ Win make_win(int32_t n, int32_t w) {
   return q;
 }
 
-// One stage on P staged lines: V (input) -> R (output), both P x LS. tot: P x 2 x TS scratch.
+// Line-sample index of extended position e in direction dir (1: the reversed line).
+__device__ __forceinline__ int32_t ext_index(int32_t e, int32_t n, int dir) {
+  const int32_t i = reflect_index(e, n);
+  return dir ? n - 1 - i : i;
+}
+
+// The fold of a chunk [c0, c1] of direction dir into acc (first sample stored as is), calling
+// f(e, local) after every sample. Interior chunks index linearly; boundary chunks reflect.
+template <class T, int OP, class F>
+__device__ __forceinline__ T fold_chunk(const T* __restrict__ V, int32_t PP, int32_t n, int32_t c0, int32_t c1,
+                                        int dir, F&& f) {
+  T loc;
+  if (c0 >= 0 && c1 <= n - 1) {
+    int32_t i = dir ? n - 1 - c0 : c0;
+    const int32_t di = dir ? -PP : PP;
+    const T* ptr = V + i * PP;
+    loc = *ptr;
+    f(c0, loc);
+    for (int32_t e = c0 + 1; e <= c1; ++e) {
+      ptr += di;
+      loc = fop<OP>(loc, *ptr);
+      f(e, loc);
+    }
+  } else {
+    loc = V[ext_index(c0, n, dir) * PP];
+    f(c0, loc);
+    for (int32_t e = c0 + 1; e <= c1; ++e) {
+      loc = fop<OP>(loc, V[ext_index(e, n, dir) * PP]);
+      f(e, loc);
+    }
+  }
+  return loc;
+}
+
+// One stage on the staged lines of this CTA: V -> R (both n x PP, line p at column p), tot: the
+// chunk totals / carries [2][TS][PP]. Workers: P lanes each (lane % P = the line).
 template <class T, int OP>
-__device__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int P, int32_t n,
-                          int32_t LS, int32_t TS, const Win& q) {
-  const int tid = threadIdx.x;
+__device__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int P, int32_t PP,
+                          int32_t n, int32_t TS, const Win& q) {
+  const int lane = threadIdx.x & 31;
+  const int slots = 32 / P;
+  const int p = lane % P;
+  const bool active_lane = lane < slots * P;
+  const int worker = (threadIdx.x >> 5) * slots + lane / P;
+  const int workers = kWarps * slots;
   const int32_t per_dir = q.nseg * q.cps;
   const int32_t e_max = n - 1 + q.r;
-  const auto ext = [&](const T* Vl, int32_t e, int dir) {
-    int32_t i = reflect_index(e, n);
-    if (dir) i = n - 1 - i;
-    return Vl[pidx(i)];
-  };
+  const T* Vp = V + p;
+  T* Rp = R + p;
   if (q.cps > 1) {
-    // phase 1: chunk totals
-    const int32_t tasks = P * 2 * per_dir;
-    for (int32_t t = tid; t < tasks; t += blockDim.x) {
-      const int32_t p = t / (2 * per_dir);
-      const int32_t rem = t - p * 2 * per_dir;
-      const int dir = rem >= per_dir;
-      const int32_t u = rem - dir * per_dir;
+    // phase 1: chunk totals of both directions
+    for (int32_t t = worker; active_lane && t < 2 * per_dir; t += workers) {
+      const int dir = t >= per_dir;
+      const int32_t u = t - dir * per_dir;
       const int32_t k = u / q.cps, c = u - k * q.cps;
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t c0 = s + 32 * c;
       if (c0 > e_last) continue;
-      const int32_t c1 = min(c0 + 31, e_last);
-      const T* Vl = V + p * LS;
-      T acc = ext(Vl, c0, dir);
-      for (int32_t e = c0 + 1; e <= c1; ++e) acc = fop<OP>(acc, ext(Vl, e, dir));
-      tot[(p * 2 + dir) * TS + u] = acc;
+      const T total = fold_chunk<T, OP>(Vp, PP, n, c0, min(c0 + 31, e_last), dir, [](int32_t, T) {});
+      tot[(dir * TS + u) * PP + p] = total;
     }
     __syncthreads();
     // phase 2: exclusive carries per segment, in place (slot c holds the carry of chunk c >= 1)
-    const int32_t segs = P * 2 * q.nseg;
-    for (int32_t t = tid; t < segs; t += blockDim.x) {
-      const int32_t p = t / (2 * q.nseg);
-      const int32_t rem = t - p * 2 * q.nseg;
-      const int dir = rem >= q.nseg;
-      const int32_t k = rem - dir * q.nseg;
+    for (int32_t t = worker; active_lane && t < 2 * q.nseg; t += workers) {
+      const int dir = t >= q.nseg;
+      const int32_t k = t - dir * q.nseg;
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t nch = (e_last - s) / 32 + 1;
-      T* tl = tot + (p * 2 + dir) * TS + k * q.cps;
+      T* tl = tot + (dir * TS + k * q.cps) * PP + p;
       T run = tl[0];
       for (int32_t c = 1; c < nch; ++c) {
-        const T next = tl[c];
-        tl[c] = run;
+        const T next = tl[c * PP];
+        tl[c * PP] = run;
         run = fop<OP>(run, next);
       }
     }
     __syncthreads();
   }
-  // phase 3 (H, dir 1) then phase 4 (G, dir 0, combined with H in place)
-  for (int dir = 1; dir >= 0; --dir) {
-    const int32_t tasks = P * per_dir;
-    for (int32_t t = tid; t < tasks; t += blockDim.x) {
-      const int32_t p = t / per_dir;
-      const int32_t u = t - p * per_dir;
-      const int32_t k = u / q.cps, c = u - k * q.cps;
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
-      const int32_t e_last = min(s + q.wa - 1, e_max);
-      const int32_t c0 = s + 32 * c;
-      if (c0 > e_last) continue;
-      const int32_t c1 = min(c0 + 31, e_last);
-      const T* Vl = V + p * LS;
-      T* Rl = R + p * LS;
-      const bool carry = c > 0;
-      const T cv = carry ? tot[(p * 2 + dir) * TS + u] : T(0);
-      T loc = T(0);
-      for (int32_t e = c0; e <= c1; ++e) {
-        const T v = ext(Vl, e, dir);
-        loc = e == c0 ? v : fop<OP>(loc, v);
-        if (e < q.r) continue;
-        const T val = carry ? fop<OP>(cv, loc) : loc;
-        if (dir) {
-          Rl[pidx(n - 1 + q.r - e)] = val;
-        } else {
-          const int32_t x = e - q.r;
-          const T h = Rl[pidx(x)];
-          if constexpr (OP == kOpSum) {
-            const T sum = add_rn(h, val);
-            Rl[pidx(x)] = e == s + q.wa - 1 ? mul_rn(sum, T(0.5)) : sum;
-          } else {
-            Rl[pidx(x)] = fop<OP>(h, val);
-          }
-        }
-      }
-    }
-    __syncthreads();
+  // phase 3: H (the reversed line's G) into R at the output slots
+  for (int32_t u = worker; active_lane && u < per_dir; u += workers) {
+    const int32_t k = u / q.cps, c = u - k * q.cps;
+    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t e_last = min(s + q.wa - 1, e_max);
+    const int32_t c0 = s + 32 * c;
+    if (c0 > e_last) continue;
+    const bool carry = c > 0;
+    const T cv = carry ? tot[(TS + u) * PP + p] : T(0);
+    fold_chunk<T, OP>(Vp, PP, n, c0, min(c0 + 31, e_last), 1, [&](int32_t e, T loc) {
+      if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = carry ? fop<OP>(cv, loc) : loc;
+    });
   }
+  __syncthreads();
+  // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r))
+  for (int32_t u = worker; active_lane && u < per_dir; u += workers) {
+    const int32_t k = u / q.cps, c = u - k * q.cps;
+    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t e_last = min(s + q.wa - 1, e_max);
+    const int32_t c0 = s + 32 * c;
+    if (c0 > e_last) continue;
+    const bool carry = c > 0;
+    const T cv = carry ? tot[u * PP + p] : T(0);
+    const int32_t e_al = s + q.wa - 1;
+    fold_chunk<T, OP>(Vp, PP, n, c0, min(c0 + 31, e_last), 0, [&](int32_t e, T loc) {
+      if (e < q.r) return;
+      const T g = carry ? fop<OP>(cv, loc) : loc;
+      T* slot = Rp + (e - q.r) * PP;
+      const T h = *slot;
+      if constexpr (OP == kOpSum) {
+        const T sum = add_rn(h, g);
+        *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+      } else {
+        *slot = fop<OP>(h, g);
+      }
+    });
+  }
+  __syncthreads();
 }
 
 template <class T>
@@ -186,8 +218,7 @@ struct PassArgs {
   int32_t last;           // the cube's last pass (box scale / epilogue)
   int32_t epi;            // BoxEpi on the last pass
   const T* aux;
-  int32_t P;
-  int64_t groups;         // line groups per element
+  int32_t P;              // lines per CTA (1, 2, 4, 8, 16 or 32)
   int32_t rung_loop;      // 1: the CTA loops over the rungs (shared input); else blockIdx.z is the rung
   unsigned long long* bytes;  // instrumentation: the pass's algorithmic bytes (nullptr: off)
 };
@@ -199,17 +230,15 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
   const int axis = a.axis;
   const int32_t n = g.n[axis];
   const bool contig = axis == g.dim - 1;
-  const int32_t LS = line_slots(n);
-  const int32_t TS = tot_slots(n);
   const int P = a.P;
+  const int32_t PP = line_pitch(P);
+  const int32_t TS = tot_slots(n);
   T* V = reinterpret_cast<T*>(smem_raw);
-  T* R = V + P * LS;
-  T* tot = R + P * LS;
-  __shared__ int64_t base_s[64];
-  __shared__ int32_t ok_s[64];
-  // the CTA's lines
+  T* R = V + static_cast<int64_t>(n) * PP;
+  T* tot = R + static_cast<int64_t>(n) * PP;
+  __shared__ int64_t base_s[32];
+  __shared__ int32_t ok_s[32];
   const int64_t grp = blockIdx.x;
-  int64_t step;
   if (threadIdx.x < P) {
     const int p = threadIdx.x;
     bool ok;
@@ -229,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
     base_s[p] = base;
     ok_s[p] = ok ? 1 : 0;
   }
-  step = contig ? 1 : g.stride[axis];
+  const int64_t step = contig ? 1 : g.stride[axis];
   __syncthreads();
   int32_t valid = 0;
   if (a.bytes && threadIdx.x == 0) {
@@ -257,7 +286,6 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
       // stage field f (the input of this rung) as values (box) or order keys (max / min)
       const bool shared_in = a.in_stride == 0 && (f == 0 || a.in1 == nullptr);
       if (!(staged && shared_in)) {
-        __syncthreads();
         const T* src = (f == 0 || a.in1 == nullptr) ? a.in0 : a.in1;
         if (src) src += static_cast<int64_t>(j) * a.in_stride + eoff;
         const uint8_t* bits = a.bits ? a.bits + eoff : nullptr;
@@ -275,16 +303,16 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
           T v;
           if (bits) v = ((bits[at] >> a.bit) & 1u) ? T(1) : T(0);
           else v = src[at];
-          V[p * LS + pidx(i)] = box ? v : okey(v);
+          V[i * PP + p] = box ? v : okey(v);
         }
         __syncthreads();
         staged = shared_in;
         acct += static_cast<unsigned long long>(valid) * n * (bits ? 1u : sizeof(T));
       }
       const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-      if (box) run_stage<T, kOpSum>(V, R, tot, P, n, LS, TS, q);
-      else if (is_min) run_stage<T, kOpMinK>(V, R, tot, P, n, LS, TS, q);
-      else run_stage<T, kOpMaxK>(V, R, tot, P, n, LS, TS, q);
+      if (box) run_stage<T, kOpSum>(V, R, tot, P, PP, n, TS, q);
+      else if (is_min) run_stage<T, kOpMinK>(V, R, tot, P, PP, n, TS, q);
+      else run_stage<T, kOpMaxK>(V, R, tot, P, PP, n, TS, q);
       // store (pads of the contiguous axis written as 0)
       T* dst = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + eoff;
       acct += static_cast<unsigned long long>(valid) * n * sizeof(T);
@@ -305,7 +333,7 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
           dst[at] = T(0);
           continue;
         }
-        T y = R[p * LS + pidx(i)];
+        T y = R[i * PP + p];
         if (!box) {
           y = okey(y);
         } else if (a.last) {
@@ -324,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
 }
 
 size_t smem_bytes(int32_t n, int P, size_t es) {
-  return (static_cast<size_t>(2) * P * line_slots(n) + static_cast<size_t>(2) * P * tot_slots(n)) * es;
+  return (static_cast<size_t>(2) * n + static_cast<size_t>(2) * tot_slots(n)) * static_cast<size_t>(line_pitch(P)) * es;
 }
 
 struct DevFacts {
@@ -343,7 +371,7 @@ DevFacts dev_facts() {
     EDAB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     EDAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     f[dev].sms = sms;
-    f[dev].smem = static_cast<size_t>(optin) - 2048;  // the kernel's static shared memory
+    f[dev].smem = static_cast<size_t>(optin) - 1024;  // the kernel's static shared memory
     EDAB_CUDA(cudaFuncSetAttribute(cube_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(f[dev].smem)));
     EDAB_CUDA(cudaFuncSetAttribute(cube_pass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(f[dev].smem)));
     have[dev] = true;
@@ -351,18 +379,19 @@ DevFacts dev_facts() {
   return f[dev];
 }
 
-// Lines per CTA: rows up to ~8192 samples per CTA; column panels of 8 to 32 lines (whole sectors).
+// Lines per CTA (a power of two up to 32): 8 lines for column panels (whole sectors, and shared
+// memory for several CTAs per SM), rows up to 8 per CTA; fewer where the shared memory or the
+// element's rows run out.
 template <class T>
 int lines_per_cta(const Geom& g, int axis, size_t cap) {
   const int32_t n = g.n[axis];
-  int P;
+  int P = 8;
   if (axis == g.dim - 1) {
-    P = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({static_cast<int64_t>(8192 / std::max(n, 1)), g.rows, 64})));
+    while (P > 1 && P / 2 >= g.rows) P /= 2;
   } else {
-    const int64_t inner = g.stride[axis];
-    P = static_cast<int>(std::min<int64_t>(32, std::max<int64_t>(1, inner)));
+    while (P > 1 && P / 2 >= g.stride[axis]) P /= 2;
   }
-  while (P > 1 && smem_bytes(n, P, sizeof(T)) > cap) --P;
+  while (P > 1 && smem_bytes(n, P, sizeof(T)) > cap / 2) P /= 2;
   if (smem_bytes(n, P, sizeof(T)) > cap) {
     throw std::invalid_argument("edab: an axis of " + std::to_string(n) + " samples exceeds the shared-memory line capacity");
   }
@@ -382,7 +411,6 @@ void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
     for (int ax = 0; ax < a.axis; ++ax) outer *= g.n[ax];
     groups = outer * ((g.stride[a.axis] + P - 1) / P);
   }
-  a.groups = groups;
   if (groups > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: cube launch too large");
   const dim3 grid(static_cast<unsigned>(groups), static_cast<unsigned>(g.batch), a.rung_loop ? 1u : static_cast<unsigned>(a.rungs));
   a.bytes = cube_bytes_counter();

@@ -74,7 +74,8 @@ __global__ void collect_kernel(int64_t B, int32_t P, int32_t cap, int64_t count,
   }
 }
 
-int32_t max_axis(int dtype) { return dtype == 0 ? 8192 : 8192; }
+// The longest axis: a cube pass stages whole lines in shared memory (the reference's limits).
+int32_t max_axis(int dtype) { return dtype == 0 ? 8192 : 4096; }
 
 }  // namespace
 

@@ -135,19 +135,23 @@ void apply_axis(cudaStream_t s, const Geom& g, int a, const T* M, const T* in, T
   EDAB_LAUNCH("gemm_simt");
 }
 
-// The element's mean in double: a fixed per-thread order and a fixed tree (one CTA per element).
+// The element's mean in double, deterministic for a shape: fixed chunks of kMeanChunk padded
+// samples, each summed by one CTA (a fixed per-thread order and a fixed tree), the chunk sums then
+// added in chunk order.
+constexpr int64_t kMeanChunk = 1 << 16;
+
 template <class T>
-__global__ void __launch_bounds__(256) mean_kernel(Geom g, const T* __restrict__ r, const int32_t* run, double* mean) {
+__global__ void __launch_bounds__(256) mean_partial(Geom g, const T* __restrict__ r, const int32_t* run, double* part,
+                                                    int64_t nchunks) {
   __shared__ double sh[256];
-  const int64_t b = blockIdx.x;
+  const int64_t b = blockIdx.y, c = blockIdx.x;
   const int32_t nl = g.n[g.dim - 1];
-  const int64_t total = g.rows * nl;
   double acc = 0.0;
   if (run[b]) {
     const T* rb = r + b * g.field;
-    for (int64_t i = threadIdx.x; i < total; i += 256) {
-      const int64_t q = i / nl;
-      acc = __dadd_rn(acc, static_cast<double>(rb[q * g.pitch + (i - q * nl)]));
+    const int64_t v1 = min(g.field, (c + 1) * kMeanChunk);
+    for (int64_t v = c * kMeanChunk + threadIdx.x; v < v1; v += 256) {
+      if (v % g.pitch < nl) acc = __dadd_rn(acc, static_cast<double>(rb[v]));
     }
   }
   sh[threadIdx.x] = acc;
@@ -156,7 +160,16 @@ __global__ void __launch_bounds__(256) mean_kernel(Geom g, const T* __restrict__
     if (threadIdx.x < st) sh[threadIdx.x] = __dadd_rn(sh[threadIdx.x], sh[threadIdx.x + st]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) mean[b] = run[b] ? __ddiv_rn(sh[0], static_cast<double>(total)) : 0.0;
+  if (threadIdx.x == 0) part[b * nchunks + c] = sh[0];
+}
+
+__global__ void mean_final(int64_t B, int64_t count, const int32_t* run, const double* part, int64_t nchunks,
+                           double* mean) {
+  const int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (b >= B) return;
+  double s = 0.0;
+  for (int64_t c = 0; c < nchunks; ++c) s = __dadd_rn(s, part[b * nchunks + c]);
+  mean[b] = run[b] ? __ddiv_rn(s, static_cast<double>(count)) : 0.0;
 }
 
 // The frequencies of DCT index k in cycles per sample (u_a = k_a / (2 n_a)) and rad = |u|.
@@ -364,9 +377,15 @@ void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T*
   T* R1 = work + 3 * F;  // D fields
   T* R2 = R1 + D * F;    // D (D + 1) / 2 fields
   // mean, then f = r - mean (the difference in double, rounded to T)
-  double* mean = reinterpret_cast<double*>(Z);  // B doubles at the head of Z, consumed before Z is used
-  mean_kernel<T><<<static_cast<unsigned>(g.batch), 256, 0, s>>>(g, r, run, mean);
-  EDAB_LAUNCH("mean_kernel");
+  // the means and the chunk sums at the head of Z, consumed before Z is used
+  const int64_t nchunks = (g.field + kMeanChunk - 1) / kMeanChunk;
+  double* mean = reinterpret_cast<double*>(Z);
+  double* part = mean + g.batch;
+  mean_partial<T><<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(g.batch)), 256, 0, s>>>(g, r, run, part,
+                                                                                                       nchunks);
+  EDAB_LAUNCH("mean_partial");
+  mean_final<<<blocks_for(g.batch), 256, 0, s>>>(g.batch, g.count, run, part, nchunks, mean);
+  EDAB_LAUNCH("mean_final");
   for_voxels(s, g, [=] __device__(int64_t b) { return run[b] != 0; },
              [=] __device__(int64_t b, int64_t, int64_t i) {
                Y[i] = static_cast<T>(__dsub_rn(static_cast<double>(r[i]), mean[b]));
