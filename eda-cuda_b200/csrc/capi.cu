@@ -51,6 +51,11 @@ void put(char* buf, size_t len, const std::string& s) {
 
 }  // namespace
 
+namespace edab {
+// The calling thread's last error message, for entry points defined in other files.
+void set_last_error(const char* message) { g_last_error = message; }
+}  // namespace edab
+
 extern "C" {
 
 int eda_decompose(const void* x, int x_on_device, int dtype, int dim, int64_t batch, const int64_t* n,

@@ -14,6 +14,7 @@ namespace edab {
 Workspace::~Workspace() { release(); }
 
 void Workspace::release() {
+  if (!owned_) return;  // a view of caller-owned memory
   if (base_) {
     int prev = -1;
     cudaGetDevice(&prev);

@@ -14,6 +14,10 @@ namespace edab {
 // A grow-only device buffer carved into 256-byte aligned slices (one per thread and device).
 class Workspace {
  public:
+  Workspace() = default;
+  // A view of caller-owned device memory: never allocates, resized or freed by the view.
+  Workspace(void* external, size_t bytes)
+      : base_(static_cast<unsigned char*>(external)), size_(bytes), owned_(false) {}
   ~Workspace();
   void reserve(size_t bytes);  // frees and reallocates when the buffer is smaller
   void reset() { used_ = 0; }
@@ -32,6 +36,7 @@ class Workspace {
   size_t size_ = 0;
   size_t used_ = 0;
   int device_ = -1;
+  bool owned_ = true;
 };
 Workspace& thread_workspace();
 
