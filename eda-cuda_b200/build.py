@@ -33,7 +33,7 @@ def sources() -> list[Path]:
 
 
 def headers() -> list[Path]:
-    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + [HERE.parent / "include" / "eda_b200.h"]
+    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + sorted((HERE.parent / "include").glob("*.h"))
 
 
 def _compile(src: Path) -> Path:

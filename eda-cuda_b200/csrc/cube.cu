@@ -18,12 +18,16 @@
 // task on their P lines, so control flow is uniform and a worker's shared-memory accesses are
 // consecutive words. The fold tasks (one per direction, segment and 32-sample chunk) are spread over
 // the CTA's workers: chunk totals, per-segment exclusive carries, then the H folds and the G folds
-// combined with them; reflection is evaluated only in the chunks that cross a line end. The first
-// pass of a cube stages its input once and runs every rung of the ladder on it (the operators'
-// rung group); later passes run one rung per CTA.
+// combined with them. P is a compile-time constant, so a whole 32-sample chunk inside the line runs
+// as an unrolled fold with immediate shared-memory offsets; only the chunks that cross a line end,
+// the window's first r samples or a segment end take the general path. A chunk without a carry
+// folds from the operation's identity (-0 for sums, the extreme keys for max / min), which changes
+// no bit of any result. The first pass of a cube stages its input once and runs every rung of the
+// ladder on it (the operators' rung group); later passes run one rung per CTA.
 #include "engine.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <mutex>
 
 namespace edab {
@@ -31,11 +35,12 @@ namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
 constexpr int kWarps = kThreads / 32;
+constexpr int kStageLoads = 8;  // global loads in flight per thread while staging lines
 
-__host__ __device__ inline int32_t tot_slots(int32_t n) { return n / 8 + 24; }
+__host__ __device__ constexpr int32_t tot_slots(int32_t n) { return n / 8 + 24; }
 // Words per staged sample row: P lines plus one (odd, so a transposed row staging of 32
 // consecutive samples hits 32 distinct banks); one line is stored contiguously.
-__host__ __device__ inline int32_t line_pitch(int P) { return P == 1 ? 1 : P + 1; }
+__host__ __device__ constexpr int32_t line_pitch(int P) { return P == 1 ? 1 : P + 1; }
 
 // Order key of v as a T-sized integer (its own inverse): integer order = order of max_c/min_c.
 __device__ __forceinline__ float okey(float v) {
@@ -64,10 +69,25 @@ __device__ __forceinline__ double fop(double a, double b) {
     return __longlong_as_double(OP == kOpMaxK ? (x > y ? x : y) : (x < y ? x : y));
   }
 }
+// The identity of fop: fop(identity, x) == x bit for bit (-0 + x == x; the extreme integer keys).
+template <class T, int OP>
+__device__ __forceinline__ T fold_identity() {
+  if constexpr (OP == kOpSum) {
+    return T(-0.0);
+  } else if constexpr (sizeof(T) == 4) {
+    return __int_as_float(OP == kOpMaxK ? INT_MIN : INT_MAX);
+  } else {
+    return __longlong_as_double(OP == kOpMaxK ? LLONG_MIN : LLONG_MAX);
+  }
+}
 
 struct Win {
   int32_t r, wa, o, k_lo, nseg, cps;
 };
+__device__ __forceinline__ int32_t geom_n(const Geom& g, int a) { return a == 0 ? g.n[0] : (a == 1 ? g.n[1] : g.n[2]); }
+__device__ __forceinline__ int64_t geom_stride(const Geom& g, int a) {
+  return a == 0 ? g.stride[0] : (a == 1 ? g.stride[1] : g.stride[2]);
+}
 __device__ __forceinline__ Win make_win(int32_t n, int32_t w) {
   Win q;
   const int32_t half = (w - 1) / 2;
@@ -87,11 +107,11 @@ __device__ __forceinline__ int32_t ext_index(int32_t e, int32_t n, int dir) {
   return dir ? n - 1 - i : i;
 }
 
-// The fold of a chunk [c0, c1] of direction dir into acc (first sample stored as is), calling
-// f(e, local) after every sample. Interior chunks index linearly; boundary chunks reflect.
+// The general fold of a chunk [c0, c1] of direction dir into acc (first sample stored as is),
+// calling f(e, local) after every sample: interior chunks index linearly, boundary chunks reflect.
 template <class T, int OP, class F>
-__device__ __forceinline__ T fold_chunk(const T* __restrict__ V, int32_t PP, int32_t n, int32_t c0, int32_t c1,
-                                        int dir, F&& f) {
+__device__ __forceinline__ T fold_chunk(const T* __restrict__ V, int32_t PP, int32_t n, int32_t c0, int32_t c1, int dir,
+                                     F&& f) {
   T loc;
   if (c0 >= 0 && c1 <= n - 1) {
     int32_t i = dir ? n - 1 - c0 : c0;
@@ -115,37 +135,107 @@ __device__ __forceinline__ T fold_chunk(const T* __restrict__ V, int32_t PP, int
   return loc;
 }
 
+// The unrolled folds of a whole 32-sample chunk inside the line (STEP: +PP forward, -PP reversed).
+template <class T, int OP, int STEP>
+__device__ __forceinline__ T chunk_total(const T* __restrict__ vp) {
+  T loc = vp[0];
+#pragma unroll
+  for (int s = 1; s < 32; ++s) loc = fop<OP>(loc, vp[s * STEP]);
+  return loc;
+}
+// H of the chunk into its output slots (one slot back per sample): carry op local.
+template <class T, int OP, int PP>
+__device__ __forceinline__ void chunk_h(const T* __restrict__ vp, T* __restrict__ rp, T cv) {
+  if constexpr (OP == kOpSum) {
+    T loc = vp[0];
+    rp[0] = add_rn(cv, loc);
+#pragma unroll
+    for (int s = 1; s < 32; ++s) {
+      loc = add_rn(loc, vp[-s * PP]);
+      rp[-s * PP] = add_rn(cv, loc);
+    }
+  } else {
+    T loc = cv;
+#pragma unroll
+    for (int s = 0; s < 32; ++s) {
+      loc = fop<OP>(loc, vp[-s * PP]);
+      rp[-s * PP] = loc;
+    }
+  }
+}
+// G of the chunk combined with the H already in its output slots; the segment's last sample of an
+// aligned box window (aligned_end) takes (H + G) * 0.5.
+template <class T, int OP, int PP>
+__device__ __forceinline__ void chunk_g(const T* __restrict__ vp, T* __restrict__ rp, T cv, bool aligned_end) {
+  if constexpr (OP == kOpSum) {
+    T loc = vp[0];
+#pragma unroll
+    for (int s = 0; s < 32; ++s) {
+      if (s) loc = add_rn(loc, vp[s * PP]);
+      const T y = add_rn(rp[s * PP], add_rn(cv, loc));
+      rp[s * PP] = (s == 31 && aligned_end) ? mul_rn(y, T(0.5)) : y;
+    }
+  } else {
+    T loc = cv;
+#pragma unroll
+    for (int s = 0; s < 32; ++s) {
+      loc = fop<OP>(loc, vp[s * PP]);
+      rp[s * PP] = fop<OP>(rp[s * PP], loc);
+    }
+  }
+}
+
 // One stage on the staged lines of this CTA: V -> R (both n x PP, line p at column p), tot: the
 // chunk totals / carries [2][TS][PP]. Workers: P lanes each (lane % P = the line).
-template <class T, int OP>
-__device__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int P, int32_t PP,
-                          int32_t n, int32_t TS, const Win& q) {
+template <class T, int OP, int P>
+__device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int32_t n, int32_t TS,
+                          const Win& q) {
+  constexpr int PP = line_pitch(P);
+  constexpr int slots = 32 / P;
+  constexpr int workers = kWarps * slots;
   const int lane = threadIdx.x & 31;
-  const int slots = 32 / P;
-  const int p = lane % P;
-  const bool active_lane = lane < slots * P;
+  const int p = lane & (P - 1);
   const int worker = (threadIdx.x >> 5) * slots + lane / P;
-  const int workers = kWarps * slots;
   const int32_t per_dir = q.nseg * q.cps;
   const int32_t e_max = n - 1 + q.r;
   const T* Vp = V + p;
   T* Rp = R + p;
+  const T idn = fold_identity<T, OP>();
+  // Tasks are enumerated chunk-major (u = c nseg + k), so the workers of a warp take the same
+  // chunk of consecutive segments (wa samples apart, spreading their shared-memory banks) rather
+  // than consecutive chunks of one segment (32 samples apart: the same banks). slot = k cps + c.
   if (q.cps > 1) {
     // phase 1: chunk totals of both directions
-    for (int32_t t = worker; active_lane && t < 2 * per_dir; t += workers) {
+    for (int32_t t = worker; t < 2 * per_dir; t += workers) {
       const int dir = t >= per_dir;
       const int32_t u = t - dir * per_dir;
-      const int32_t k = u / q.cps, c = u - k * q.cps;
+      const int32_t c = u / q.nseg, k = u - c * q.nseg;
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t c0 = s + 32 * c;
       if (c0 > e_last) continue;
-      const T total = fold_chunk<T, OP>(Vp, PP, n, c0, min(c0 + 31, e_last), dir, [](int32_t, T) {});
-      tot[(dir * TS + u) * PP + p] = total;
+      const int32_t c1 = min(c0 + 31, e_last);
+      T total;
+      if (c0 >= 0 && c1 <= n - 1) {
+        const T* vp = Vp + (dir ? n - 1 - c0 : c0) * PP;
+        if (c1 == c0 + 31) {
+          total = dir ? chunk_total<T, OP, -PP>(vp) : chunk_total<T, OP, PP>(vp);
+        } else {
+          const int32_t step = dir ? -PP : PP;
+          total = *vp;
+          for (int32_t e = c0 + 1; e <= c1; ++e) {
+            vp += step;
+            total = fop<OP>(total, *vp);
+          }
+        }
+      } else {
+        total = fold_chunk<T, OP>(Vp, PP, n, c0, c1, dir, [](int32_t, T) {});
+      }
+      tot[(dir * TS + k * q.cps + c) * PP + p] = total;
     }
     __syncthreads();
     // phase 2: exclusive carries per segment, in place (slot c holds the carry of chunk c >= 1)
-    for (int32_t t = worker; active_lane && t < 2 * q.nseg; t += workers) {
+    for (int32_t t = worker; t < 2 * q.nseg; t += workers) {
       const int dir = t >= q.nseg;
       const int32_t k = t - dir * q.nseg;
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
@@ -161,42 +251,90 @@ __device__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restr
     }
     __syncthreads();
   }
-  // phase 3: H (the reversed line's G) into R at the output slots
-  for (int32_t u = worker; active_lane && u < per_dir; u += workers) {
-    const int32_t k = u / q.cps, c = u - k * q.cps;
+  // phase 3: H (the reversed line's G) into R at the output slots n - 1 + r - e (e >= r)
+  for (int32_t u = worker; u < per_dir; u += workers) {
+    const int32_t c = u / q.nseg, k = u - c * q.nseg;
     const int32_t s = q.o + (q.k_lo + k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
     const int32_t c0 = s + 32 * c;
     if (c0 > e_last) continue;
-    const bool carry = c > 0;
-    const T cv = carry ? tot[(TS + u) * PP + p] : T(0);
-    fold_chunk<T, OP>(Vp, PP, n, c0, min(c0 + 31, e_last), 1, [&](int32_t e, T loc) {
-      if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = carry ? fop<OP>(cv, loc) : loc;
-    });
+    const int32_t c1 = min(c0 + 31, e_last);
+    const T cv = c > 0 ? tot[(TS + k * q.cps + c) * PP + p] : idn;
+    if (c0 >= 0 && c1 <= n - 1) {
+      const T* vp = Vp + (n - 1 - c0) * PP;
+      if (c1 == c0 + 31 && c0 >= q.r) {
+        chunk_h<T, OP, PP>(vp, Rp + (n - 1 + q.r - c0) * PP, cv);
+      } else {
+        // first output at e = max(c0, r); slots step back one sample per sample
+        const int32_t e_out = max(c0, q.r);
+        T* rp = Rp + (n - 1 + q.r - e_out) * PP;
+        T loc = OP == kOpSum ? *vp : fop<OP>(cv, *vp);
+        for (int32_t e = c0; e <= c1; ++e) {
+          if (e > c0) {
+            vp -= PP;
+            loc = fop<OP>(loc, *vp);
+          }
+          if (e >= e_out) {
+            *rp = OP == kOpSum ? add_rn(cv, loc) : loc;
+            rp -= PP;
+          }
+        }
+      }
+    } else {
+      fold_chunk<T, OP>(Vp, PP, n, c0, c1, 1, [&](int32_t e, T loc) {
+        if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = fop<OP>(cv, loc);
+      });
+    }
   }
   __syncthreads();
-  // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r))
-  for (int32_t u = worker; active_lane && u < per_dir; u += workers) {
-    const int32_t k = u / q.cps, c = u - k * q.cps;
+  // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r)), slot x = e - r
+  for (int32_t u = worker; u < per_dir; u += workers) {
+    const int32_t c = u / q.nseg, k = u - c * q.nseg;
     const int32_t s = q.o + (q.k_lo + k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
     const int32_t c0 = s + 32 * c;
     if (c0 > e_last) continue;
-    const bool carry = c > 0;
-    const T cv = carry ? tot[u * PP + p] : T(0);
+    const int32_t c1 = min(c0 + 31, e_last);
+    const T cv = c > 0 ? tot[(k * q.cps + c) * PP + p] : idn;
     const int32_t e_al = s + q.wa - 1;
-    fold_chunk<T, OP>(Vp, PP, n, c0, min(c0 + 31, e_last), 0, [&](int32_t e, T loc) {
-      if (e < q.r) return;
-      const T g = carry ? fop<OP>(cv, loc) : loc;
-      T* slot = Rp + (e - q.r) * PP;
-      const T h = *slot;
-      if constexpr (OP == kOpSum) {
-        const T sum = add_rn(h, g);
-        *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+    if (c0 >= 0 && c1 <= n - 1) {
+      const T* vp = Vp + c0 * PP;
+      if (c1 == c0 + 31 && c0 >= q.r) {
+        chunk_g<T, OP, PP>(vp, Rp + (c0 - q.r) * PP, cv, c1 == e_al);
       } else {
-        *slot = fop<OP>(h, g);
+        const int32_t e_out = max(c0, q.r);
+        T* rp = Rp + (e_out - q.r) * PP;
+        T loc = OP == kOpSum ? *vp : fop<OP>(cv, *vp);
+        for (int32_t e = c0; e <= c1; ++e) {
+          if (e > c0) {
+            vp += PP;
+            loc = fop<OP>(loc, *vp);
+          }
+          if (e >= e_out) {
+            if constexpr (OP == kOpSum) {
+              const T y = add_rn(*rp, add_rn(cv, loc));
+              *rp = e == e_al ? mul_rn(y, T(0.5)) : y;
+            } else {
+              *rp = fop<OP>(*rp, loc);
+            }
+            rp += PP;
+          }
+        }
       }
-    });
+    } else {
+      fold_chunk<T, OP>(Vp, PP, n, c0, c1, 0, [&](int32_t e, T loc) {
+        if (e < q.r) return;
+        const T g = fop<OP>(cv, loc);
+        T* slot = Rp + (e - q.r) * PP;
+        const T h = *slot;
+        if constexpr (OP == kOpSum) {
+          const T sum = add_rn(h, g);
+          *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+        } else {
+          *slot = fop<OP>(h, g);
+        }
+      });
+    }
   }
   __syncthreads();
 }
@@ -218,20 +356,32 @@ struct PassArgs {
   int32_t last;           // the cube's last pass (box scale / epilogue)
   int32_t epi;            // BoxEpi on the last pass
   const T* aux;
-  int32_t P;              // lines per CTA (1, 2, 4, 8, 16 or 32)
   int32_t rung_loop;      // 1: the CTA loops over the rungs (shared input); else blockIdx.z is the rung
   unsigned long long* bytes;  // instrumentation: the pass's algorithmic bytes (nullptr: off)
 };
 
-template <class T>
-__global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
+// Thread roles of the staging and the store of P lines of n samples. Rows (the contiguous axis):
+// warps take lines (kWarps / P warps per line when P < kWarps), lanes consecutive samples. Column
+// panels: thread t takes line t % P and samples t / P + k kThreads / P.
+template <int P>
+struct LineRoles {
+  static constexpr int kWpl = P >= kWarps ? 1 : kWarps / P;  // warps per line (rows)
+  static constexpr int kRowStride = 32 * kWpl;                 // sample stride of a thread (rows)
+  static constexpr int kColStride = kThreads / P;              // sample stride of a thread (columns)
+};
+
+template <class T, int P>
+__global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) {
+  constexpr int PP = line_pitch(P);
+  using Roles = LineRoles<P>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int64_t b = blockIdx.y;
   const int axis = a.axis;
-  const int32_t n = g.n[axis];
+  // (a kernel parameter indexed by a runtime value would be copied to local memory)
+  const int32_t n = geom_n(g, axis);
+  const int64_t axis_stride = geom_stride(g, axis);
+  const int32_t n_last = geom_n(g, g.dim - 1);
   const bool contig = axis == g.dim - 1;
-  const int P = a.P;
-  const int32_t PP = line_pitch(P);
   const int32_t TS = tot_slots(n);
   T* V = reinterpret_cast<T*>(smem_raw);
   T* R = V + static_cast<int64_t>(n) * PP;
@@ -248,17 +398,17 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
       ok = row < g.rows;
       base = row * g.pitch;
     } else {
-      const int64_t inner = g.stride[axis];
+      const int64_t inner = axis_stride;
       const int64_t gpo = (inner + P - 1) / P;
       const int64_t o = grp / gpo;
       const int64_t c = (grp - o * gpo) * P + p;
-      ok = c < inner && (c % g.pitch) < g.n[g.dim - 1];
+      ok = c < inner && (c % g.pitch) < n_last;
       base = o * static_cast<int64_t>(n) * inner + c;
     }
     base_s[p] = base;
     ok_s[p] = ok ? 1 : 0;
   }
-  const int64_t step = contig ? 1 : g.stride[axis];
+  const int64_t step = contig ? 1 : axis_stride;
   __syncthreads();
   int32_t valid = 0;
   if (a.bytes && threadIdx.x == 0) {
@@ -268,7 +418,13 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
   const int64_t eoff = b * g.field;
   const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
   const bool box = a.op == static_cast<int>(CubeOp::kBox);
-  const int32_t total = P * n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this thread's line and first sample in the staging and the store
+  const int my_p = contig ? warp / Roles::kWpl : (threadIdx.x & (P - 1));
+  const int32_t my_i0 = contig ? lane + 32 * (warp % Roles::kWpl) : static_cast<int32_t>(threadIdx.x / P);
+  const int32_t my_di = contig ? Roles::kRowStride : Roles::kColStride;
+  const int my_dp = contig ? kWarps / Roles::kWpl : P;  // line stride of this thread (rows: P > kWarps)
+  const int32_t nw = contig ? static_cast<int32_t>(g.pitch) : n;  // samples written per line
   const int32_t j_begin = a.rung_loop ? 0 : static_cast<int32_t>(blockIdx.z);
   const int32_t j_end = a.rung_loop ? a.rungs : j_begin + 1;
   bool staged = false;  // V holds the staged shared input (first pass with a rung loop)
@@ -279,7 +435,10 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
     double fac = 1.0;
     if (box && a.last) {
       double prod = 1.0;
-      for (int ax = 0; ax < g.dim; ++ax) prod *= static_cast<double>(2 * min((w - 1) / 2, g.n[ax] - 1) + 1);
+#pragma unroll
+      for (int ax = 0; ax < kMaxDim; ++ax) {
+        if (ax < g.dim) prod *= static_cast<double>(2 * min((w - 1) / 2, g.n[ax] - 1) + 1);
+      }
       fac = static_cast<double>(static_cast<T>(1.0 / prod));
     }
     for (int f = 0; f < nf; ++f) {
@@ -289,61 +448,61 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
         const T* src = (f == 0 || a.in1 == nullptr) ? a.in0 : a.in1;
         if (src) src += static_cast<int64_t>(j) * a.in_stride + eoff;
         const uint8_t* bits = a.bits ? a.bits + eoff : nullptr;
-        for (int32_t t = threadIdx.x; t < total; t += blockDim.x) {
-          int p, i;
-          if (contig) {
-            p = t / n;
-            i = t - p * n;
-          } else {
-            i = t / P;
-            p = t - i * P;
-          }
+        for (int p = my_p; p < P; p += my_dp) {
           if (!ok_s[p]) continue;
-          const int64_t at = base_s[p] + static_cast<int64_t>(i) * step;
-          T v;
-          if (bits) v = ((bits[at] >> a.bit) & 1u) ? T(1) : T(0);
-          else v = src[at];
-          V[i * PP + p] = box ? v : okey(v);
+          const int64_t base = base_s[p];
+          // kStageLoads independent loads in flight per thread before their shared-memory stores
+          for (int32_t i0 = my_i0; i0 < n; i0 += kStageLoads * my_di) {
+            T v[kStageLoads];
+#pragma unroll
+            for (int u = 0; u < kStageLoads; ++u) {
+              const int32_t i = i0 + u * my_di;
+              if (i < n) {
+                const int64_t at = base + static_cast<int64_t>(i) * step;
+                v[u] = bits ? (((bits[at] >> a.bit) & 1u) ? T(1) : T(0)) : src[at];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < kStageLoads; ++u) {
+              const int32_t i = i0 + u * my_di;
+              if (i < n) V[i * PP + p] = box ? v[u] : okey(v[u]);
+            }
+          }
         }
         __syncthreads();
         staged = shared_in;
         acct += static_cast<unsigned long long>(valid) * n * (bits ? 1u : sizeof(T));
       }
       const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-      if (box) run_stage<T, kOpSum>(V, R, tot, P, PP, n, TS, q);
-      else if (is_min) run_stage<T, kOpMinK>(V, R, tot, P, PP, n, TS, q);
-      else run_stage<T, kOpMaxK>(V, R, tot, P, PP, n, TS, q);
+      if (box) run_stage<T, kOpSum, P>(V, R, tot, n, TS, q);
+      else if (is_min) run_stage<T, kOpMinK, P>(V, R, tot, n, TS, q);
+      else run_stage<T, kOpMaxK, P>(V, R, tot, n, TS, q);
       // store (pads of the contiguous axis written as 0)
       T* dst = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + eoff;
       acct += static_cast<unsigned long long>(valid) * n * sizeof(T);
-      const int32_t nw = contig ? static_cast<int32_t>(g.pitch) : n;
-      const int32_t tw = P * nw;
-      for (int32_t t = threadIdx.x; t < tw; t += blockDim.x) {
-        int p, i;
-        if (contig) {
-          p = t / nw;
-          i = t - p * nw;
-        } else {
-          i = t / P;
-          p = t - i * P;
-        }
+      const bool detsq = box && a.last && a.epi == static_cast<int>(BoxEpi::kDetSq);
+      const T* aux = detsq ? a.aux + eoff : nullptr;
+      for (int p = my_p; p < P; p += my_dp) {
         if (!ok_s[p]) continue;
-        const int64_t at = base_s[p] + static_cast<int64_t>(i) * step;
-        if (i >= n) {
-          dst[at] = T(0);
-          continue;
-        }
-        T y = R[i * PP + p];
-        if (!box) {
-          y = okey(y);
-        } else if (a.last) {
-          y = mul_rn(y, static_cast<T>(fac));
-          if (a.epi == static_cast<int>(BoxEpi::kDetSq)) {
-            const T d = sub_rn(a.aux[eoff + at], y);
-            y = mul_rn(d, d);
+        const int64_t base = base_s[p];
+        for (int32_t i = my_i0; i < nw; i += my_di) {
+          const int64_t at = base + static_cast<int64_t>(i) * step;
+          if (i >= n) {
+            dst[at] = T(0);
+            continue;
           }
+          T y = R[i * PP + p];
+          if (!box) {
+            y = okey(y);
+          } else if (a.last) {
+            y = mul_rn(y, static_cast<T>(fac));
+            if (detsq) {
+              const T d = sub_rn(aux[at], y);
+              y = mul_rn(d, d);
+            }
+          }
+          dst[at] = y;
         }
-        dst[at] = y;
       }
       __syncthreads();  // the next stage rewrites R and tot
     }
@@ -353,6 +512,16 @@ __global__ void __launch_bounds__(kThreads) cube_pass(Geom g, PassArgs<T> a) {
 
 size_t smem_bytes(int32_t n, int P, size_t es) {
   return (static_cast<size_t>(2) * n + static_cast<size_t>(2) * tot_slots(n)) * static_cast<size_t>(line_pitch(P)) * es;
+}
+
+template <class T>
+void allow_smem(int bytes) {
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
 struct DevFacts {
@@ -372,8 +541,8 @@ DevFacts dev_facts() {
     EDAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     f[dev].sms = sms;
     f[dev].smem = static_cast<size_t>(optin) - 1024;  // the kernel's static shared memory
-    EDAB_CUDA(cudaFuncSetAttribute(cube_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(f[dev].smem)));
-    EDAB_CUDA(cudaFuncSetAttribute(cube_pass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(f[dev].smem)));
+    allow_smem<float>(static_cast<int>(f[dev].smem));
+    allow_smem<double>(static_cast<int>(f[dev].smem));
     have[dev] = true;
   }
   return f[dev];
@@ -402,7 +571,6 @@ template <class T>
 void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   const DevFacts f = dev_facts();
   const int P = lines_per_cta<T>(g, a.axis, f.smem);
-  a.P = P;
   int64_t groups;
   if (a.axis == g.dim - 1) {
     groups = (g.rows + P - 1) / P;
@@ -413,9 +581,17 @@ void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   }
   if (groups > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: cube launch too large");
   const dim3 grid(static_cast<unsigned>(groups), static_cast<unsigned>(g.batch), a.rung_loop ? 1u : static_cast<unsigned>(a.rungs));
+  const size_t smem = smem_bytes(g.n[a.axis], P, sizeof(T));
   a.bytes = cube_bytes_counter();
   profile_cube_launch(s, true);
-  cube_pass<T><<<grid, kThreads, smem_bytes(g.n[a.axis], P, sizeof(T)), s>>>(g, a);
+  switch (P) {
+    case 1: cube_pass<T, 1><<<grid, kThreads, smem, s>>>(g, a); break;
+    case 2: cube_pass<T, 2><<<grid, kThreads, smem, s>>>(g, a); break;
+    case 4: cube_pass<T, 4><<<grid, kThreads, smem, s>>>(g, a); break;
+    case 8: cube_pass<T, 8><<<grid, kThreads, smem, s>>>(g, a); break;
+    case 16: cube_pass<T, 16><<<grid, kThreads, smem, s>>>(g, a); break;
+    default: cube_pass<T, 32><<<grid, kThreads, smem, s>>>(g, a); break;
+  }
   EDAB_LAUNCH("cube_pass");
   profile_cube_launch(s, false);
 }

@@ -321,31 +321,53 @@ __global__ void __launch_bounds__(kThreads) weights_kernel(Geom g, Ctl c, const 
 // segment points (D >= 2), at x +- (i / 2) o by D-linear interpolation of the reflected periodic
 // extension. OP 0: max (Dil), 2: max and min (Dil, Ero), 3: box (Avg). The rung cubes of every rung
 // lie in rung0 (rung1: the min cubes) at j * B * field.
+// The four segment points x + (1/2) o, x - (1/2) o, x + o, x - o of a voxel (in this order): per
+// point and axis the offsets (in the element, reflected) of the two interpolation neighbours and
+// their weights. Computed once per voxel and shared by both rungs and both cubes of the gather.
 template <class T, int D>
-__device__ __forceinline__ T interp_read(const Geom& g, const T* __restrict__ f, const double* y) {
-  int64_t off0[D], off1[D];
-  T w0[D], w1[D];
+struct SegPoints {
+  int32_t off0[4][D], off1[4][D];
+  T w0[4][D], w1[4][D];
+};
+template <class T, int D>
+__device__ __forceinline__ void seg_points(const Geom& g, const int32_t* x, const double* ov, SegPoints<T, D>& P) {
 #pragma unroll
-  for (int a = 0; a < D; ++a) {
-    const double fl = floor(y[a]);
-    const double tt = __dsub_rn(y[a], fl);
-    const int64_t i0 = static_cast<int64_t>(fl);
-    const T t1 = static_cast<T>(tt);
-    w1[a] = t1;
-    w0[a] = sub_rn(T(1), t1);
-    const int64_t st = a == g.dim - 1 ? 1 : g.stride[a];
-    off0[a] = reflect_any(i0, g.n[a]) * st;
-    off1[a] = reflect_any(i0 + 1, g.n[a]) * st;
+  for (int i = 1; i <= 2; ++i) {
+    const double s = static_cast<double>(i) / 2.0;
+#pragma unroll
+    for (int sg = 0; sg < 2; ++sg) {
+      const int q = 2 * (i - 1) + sg;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const double off = __dmul_rn(s, ov[a]);
+        const double xa = static_cast<double>(x[a]);
+        const double y = sg == 0 ? __dadd_rn(xa, off) : __dsub_rn(xa, off);
+        const double fl = floor(y);
+        const double tt = __dsub_rn(y, fl);
+        const int64_t i0 = static_cast<int64_t>(fl);
+        const T t1 = static_cast<T>(tt);
+        P.w1[q][a] = t1;
+        P.w0[q][a] = sub_rn(T(1), t1);
+        const int64_t st = a == g.dim - 1 ? 1 : g.stride[a];
+        P.off0[q][a] = static_cast<int32_t>(reflect_any(i0, g.n[a]) * st);
+        P.off1[q][a] = static_cast<int32_t>(reflect_any(i0 + 1, g.n[a]) * st);
+      }
+    }
   }
+}
+// The D-linear interpolation of f at point q: corners in binary order (axis 0 the high bit), each
+// corner's value times its axis weights in axis order, summed in corner order.
+template <class T, int D>
+__device__ __forceinline__ T interp_read(const T* __restrict__ f, const SegPoints<T, D>& P, int q) {
   T acc = T(0);
 #pragma unroll
   for (int corner = 0; corner < (1 << D); ++corner) {
-    int64_t off = 0;
+    int32_t off = 0;
 #pragma unroll
-    for (int a = 0; a < D; ++a) off += ((corner >> (D - 1 - a)) & 1) ? off1[a] : off0[a];
+    for (int a = 0; a < D; ++a) off += ((corner >> (D - 1 - a)) & 1) ? P.off1[q][a] : P.off0[q][a];
     T term = __ldg(f + off);
 #pragma unroll
-    for (int a = 0; a < D; ++a) term = mul_rn(term, ((corner >> (D - 1 - a)) & 1) ? w1[a] : w0[a]);
+    for (int a = 0; a < D; ++a) term = mul_rn(term, ((corner >> (D - 1 - a)) & 1) ? P.w1[q][a] : P.w0[q][a]);
     acc = add_rn(acc, term);
   }
   return acc;
@@ -373,6 +395,8 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Geom g, const Elem* __
       const T tt = __ldg(t + at);
       const T wl = sub_rn(T(1), tt);
       T r0 = T(0), r1 = T(0);
+      SegPoints<T, (D >= 2 ? D : 1)> P;
+      bool have_pts = false;
       for (int side = 0; side < 2; ++side) {
         const int j = l + side;
         const T wgt = side == 0 ? wl : tt;
@@ -381,34 +405,29 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Geom g, const Elem* __
         const T* f1 = OP == 2 ? rung1 + static_cast<int64_t>(j) * fe + b * g.field : nullptr;
         T acc0 = __ldg(f0 + v);
         T acc1 = OP == 2 ? __ldg(f1 + v) : T(0);
-        if (D >= 2 && ((pts_mask >> j) & 1u)) {
-          double ov[kMaxDim] = {0, 0, 0};
-          ov[0] = static_cast<double>(__ldg(o0 + at));
-          if (D >= 2) ov[1] = static_cast<double>(__ldg(o1 + at));
-          if (D >= 3) ov[2] = static_cast<double>(__ldg(o2 + at));
+        if constexpr (D >= 2) {
+          if ((pts_mask >> j) & 1u) {
+            if (!have_pts) {
+              double ov[D];
+              ov[0] = static_cast<double>(__ldg(o0 + at));
+              ov[1] = static_cast<double>(__ldg(o1 + at));
+              if constexpr (D >= 3) ov[2] = static_cast<double>(__ldg(o2 + at));
+              seg_points<T, D>(g, x, ov, P);
+              have_pts = true;
+            }
 #pragma unroll
-          for (int i = 1; i <= 2; ++i) {
-            const double s = static_cast<double>(i) / 2.0;
-#pragma unroll
-            for (int sg = 0; sg < 2; ++sg) {
-              double y[kMaxDim];
-#pragma unroll
-              for (int a = 0; a < D; ++a) {
-                const double off = __dmul_rn(s, ov[a]);
-                const double xa = static_cast<double>(x[a]);
-                y[a] = sg == 0 ? __dadd_rn(xa, off) : __dsub_rn(xa, off);
-              }
+            for (int q = 0; q < 4; ++q) {
               if constexpr (OP == 2) {
-                acc0 = max_c(acc0, interp_read<T, D>(g, f0, y));
-                acc1 = min_c(acc1, interp_read<T, D>(g, f1, y));
+                acc0 = max_c(acc0, interp_read<T, D>(f0, P, q));
+                acc1 = min_c(acc1, interp_read<T, D>(f1, P, q));
               } else if constexpr (OP == 0) {
-                acc0 = max_c(acc0, interp_read<T, D>(g, f0, y));
+                acc0 = max_c(acc0, interp_read<T, D>(f0, P, q));
               } else {
-                acc0 = add_rn(acc0, interp_read<T, D>(g, f0, y));
+                acc0 = add_rn(acc0, interp_read<T, D>(f0, P, q));
               }
             }
+            if constexpr (OP == 3) acc0 = div_rn(acc0, T(5));
           }
-          if constexpr (OP == 3) acc0 = div_rn(acc0, T(5));
         }
         const T v0 = mul_rn(wgt, acc0);
         const bool add = side == 1 && wl > T(0);
@@ -499,7 +518,8 @@ class Engine {
   double* dsc_;      // 8 [B] doubles
   int64_t* cnt_;     // [B]
   uint64_t* nonfin_; // [B]
-  int32_t* any_;     // device flags
+  int32_t* any_;     // device flags: [0, 2) the mode loop's, [kTcErr] the orientation's pipeline error
+  static constexpr int kTcErr = 4;
   void* sel_ws_;
   void* tot_ws_;
   const OrientPlan* plan_ = nullptr;
@@ -552,7 +572,7 @@ void Engine<T>::bind(Workspace& ws) {
   e_ = fld(); q_ = fld(); Mn_ = fld(); u2_ = fld(); l2_ = fld(); hn_ = fld();
   rung0_ = ws.take<T>(F * kMaxRungs);
   rung1_ = ws.take<T>(F * kMaxRungs);
-  owork_ = g_.dim >= 2 ? ws.take<T>(F * orient_work_fields(g_.dim)) : nullptr;
+  owork_ = g_.dim >= 2 ? ws.take<T>(static_cast<size_t>(orient_work_samples(g_))) : nullptr;
   flags_ = ws.take<uint8_t>(F); ff_ = ws.take<uint8_t>(F); P_[0] = ws.take<uint8_t>(F); P_[1] = ws.take<uint8_t>(F);
   Pacc_ = ws.take<uint8_t>(F); A_ = ws.take<uint8_t>(F); lo_ = ws.take<uint8_t>(F); marks_ = ws.take<uint8_t>(F);
   selm_ = ws.take<uint8_t>(F);
@@ -969,7 +989,7 @@ void Engine<T>::orientation_and_build() {
   int32_t* mask_s = mask_;
   const int64_t B = B_;
   if (g_.dim >= 2) {
-    orientation<T>(s_, g_, *plan_, r_, el_, on, n_, coh_, owork_, c_.two_sigma2);
+    orientation<T>(s_, g_, *plan_, r_, el_, on, n_, coh_, owork_, c_.two_sigma2, any_ + kTcErr);
     for_elements(s_, B_, [=] __device__(int64_t b) {
       if (el[b].status == kActive && el[b].nonfinite) fail2(el[b], win_s, mask_s, B, b);
     });
@@ -1048,6 +1068,8 @@ void Engine<T>::op(int which, const T* in, T* out0, T* out1, int32_t nrm) {
   a.rungs = nrm;
   a.out_stride = B_ * g_.field;
   const CubeOp cop = which == 3 ? CubeOp::kBox : (which == 2 ? CubeOp::kMaxMin : CubeOp::kMax);
+  // the gather's segment points index an element with 32-bit offsets
+  if (g_.field > INT32_MAX) throw std::invalid_argument("eda: an element of more than 2^31 padded samples");
   cube<T>(s_, g_, cop, a);
   const dim3 grid = voxel_grid(g_);
   const int32_t* on = mask(kOn);
@@ -1317,6 +1339,7 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
   });
   EDAB_CUDA(cudaMemsetAsync(nonfin_, 0, sizeof(uint64_t) * B_, s_));
   EDAB_CUDA(cudaMemsetAsync(el_, 0, sizeof(Elem) * B_, s_));
+  EDAB_CUDA(cudaMemsetAsync(any_ + kTcErr, 0, sizeof(int32_t), s_));
   double* am = dsc_ + 2 * B_;
   double* en = dsc_ + 1 * B_;
   field_totals<T>(s_, g_, r_, en, am, nonfin_, tot_ws_);
@@ -1533,7 +1556,13 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
   }
   out.resize(static_cast<size_t>(B_));
   EDAB_CUDA(cudaMemcpyAsync(out.data(), el_, sizeof(Elem) * B_, cudaMemcpyDeviceToHost, s_));
+  int32_t tc_err = 0;
+  EDAB_CUDA(cudaMemcpyAsync(&tc_err, any_ + kTcErr, sizeof tc_err, cudaMemcpyDeviceToHost, s_));
   EDAB_CUDA(cudaStreamSynchronize(s_));
+  if (tc_err) {
+    throw CudaError("eda: a tensor-core transform of the orientation gave up waiting for its pipeline",
+                    static_cast<int>(cudaErrorLaunchTimeout));
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1541,8 +1570,9 @@ template <class T>
 size_t engine_bytes(const Geom& g) {
   const size_t F = static_cast<size_t>(g.batch * g.field);
   const int D = g.dim;
-  size_t fields = 11 + 1 + 24 + (D >= 2 ? 2 * D + orient_work_fields(D) : 0);
+  size_t fields = 11 + 1 + 24 + (D >= 2 ? 2 * D : 0);
   size_t b = fields * F * sizeof(T) + 2 * kMaxRungs * F * sizeof(T) + 9 * F + 4 * F;
+  if (D >= 2) b += static_cast<size_t>(orient_work_samples(g)) * sizeof(T);
   b += static_cast<size_t>(g.batch) * (sizeof(Elem) + 4 * (kSlots + kMasks + kMaxRungs) + 8 * 10 + 64);
   b += select_scratch_bytes(g) + totals_scratch_bytes(g);
   b += 160 * 256;  // every take is rounded up to 256 bytes

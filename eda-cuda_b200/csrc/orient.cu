@@ -1,12 +1,16 @@
 // SPDX-License-Identifier: Apache-2.0
 // The orientation (orient.cuh): mean, forward DCT-II along every axis, the log-Gabor band, the
 // Riesz components by inverse cosine / sine transforms, the energy tensor and the Jacobi
-// eigen-decomposition. The axis transforms are batched matrix products; this file holds the
-// portable SIMT product (tiled in shared memory, FP32 accumulation for float32 and FP64 for
-// float64) that the tensor-core path (orient_tc.cu) is checked against.
+// eigen-decomposition. Every axis transform is a rotated pass (RotPass): the contiguous axis of the
+// current layout is transformed and becomes the slowest axis, so D passes return a field to the
+// element layout and every pass reads K-major rows. Float32 passes run on the tensor cores
+// (orient_tc.cu, 3xTF32); float64 passes run the SIMT product below (FP64 accumulation).
 #include "orient.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <type_traits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -84,54 +88,70 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmDesc d, const T* __restrict
   }
 }
 
-// out = M applied along axis a of every element of `in` (padded fields): out[.., i, ..] =
-// sum_k M[i][k] in[.., k, ..].
+// The layout of an element's field during the orientation: axis order, the last contiguous (padded
+// to a multiple of 32 samples).
+struct Layout {
+  int dim;
+  int ax[kMaxDim];
+};
+inline int64_t pad32(int64_t n) { return (n + 31) / 32 * 32; }
+Layout element_layout(const Geom& g) {
+  Layout L{g.dim, {0, 1, 2}};
+  return L;
+}
+Layout rotated(const Layout& L) {
+  Layout R = L;
+  R.ax[0] = L.ax[L.dim - 1];
+  for (int i = 1; i < L.dim; ++i) R.ax[i] = L.ax[i - 1];
+  return R;
+}
+int64_t layout_field(const Geom& g, const Layout& L) {
+  int64_t rows = 1;
+  for (int i = 0; i < L.dim - 1; ++i) rows *= g.n[L.ax[i]];
+  return rows * pad32(g.n[L.ax[L.dim - 1]]);
+}
+RotPass make_pass(const Geom& g, const Layout& L) {
+  const int D = L.dim;
+  RotPass p{};
+  p.K = g.n[L.ax[D - 1]];
+  p.pitch_in = pad32(p.K);
+  p.rows = 1;
+  for (int i = 0; i < D - 1; ++i) p.rows *= g.n[L.ax[i]];
+  p.f_in = p.rows * p.pitch_in;
+  p.n_lo = g.n[L.ax[D - 2]];
+  p.pitch_out = pad32(p.n_lo);
+  p.s_j = (p.rows / p.n_lo) * p.pitch_out;
+  p.f_out = static_cast<int64_t>(p.K) * p.s_j;
+  p.M = g.batch * p.rows;
+  return p;
+}
+
+// The rotated pass with the SIMT product: per element and outer block o (the rows above the
+// fastest row axis), C(i, j) = sum_k A(i, k) B(k, j) with A the n_lo rows, B(k, j) = M[j][k].
 template <class T>
-void apply_axis(cudaStream_t s, const Geom& g, int a, const T* M, const T* in, T* out, const int32_t* run) {
+void rot_pass_simt(cudaStream_t s, const RotPass& p, int32_t n, const T* M, const T* in, T* out, const int32_t* run) {
   GemmDesc d{};
-  const int64_t n = g.n[a];
-  if (a == g.dim - 1) {
-    // rows x n times M^T
-    d.M = g.rows;
-    d.N = n;
-    d.K = n;
-    d.sAi = g.pitch;
-    d.sAk = 1;
-    d.sBk = 1;
-    d.sBj = n;
-    d.sCi = g.pitch;
-    d.sCj = 1;
-    d.outer = 1;
-    d.eA = g.field;
-    d.eB = 0;
-    d.eC = g.field;
-    const dim3 grid(static_cast<unsigned>((d.N + kBN - 1) / kBN), static_cast<unsigned>((d.M + kBM - 1) / kBM),
-                    static_cast<unsigned>(g.batch));
-    gemm_simt<T><<<grid, 256, 0, s>>>(d, in, M, out, run);
-  } else {
-    const int64_t inner = g.stride[a];
-    int64_t outer = 1;
-    for (int ax = 0; ax < a; ++ax) outer *= g.n[ax];
-    d.M = n;
-    d.N = inner;
-    d.K = n;
-    d.sAi = n;
-    d.sAk = 1;
-    d.sBk = inner;
-    d.sBj = 1;
-    d.sCi = inner;
-    d.sCj = 1;
-    d.outer = outer;
-    d.eA = 0;
-    d.oA = 0;
-    d.eB = g.field;
-    d.oB = n * inner;
-    d.eC = g.field;
-    d.oC = n * inner;
-    const dim3 grid(static_cast<unsigned>((d.N + kBN - 1) / kBN), static_cast<unsigned>((d.M + kBM - 1) / kBM),
-                    static_cast<unsigned>(g.batch * outer));
-    gemm_simt<T><<<grid, 256, 0, s>>>(d, M, in, out, run);
-  }
+  const int64_t outer = p.rows / p.n_lo;
+  d.M = p.n_lo;
+  d.N = p.K;
+  d.K = p.K;
+  d.sAi = p.pitch_in;
+  d.sAk = 1;
+  d.sBk = 1;
+  d.sBj = n;
+  d.sCi = 1;
+  d.sCj = p.s_j;
+  d.outer = outer;
+  d.eA = p.f_in;
+  d.oA = p.n_lo * p.pitch_in;
+  d.eB = 0;
+  d.oB = 0;
+  d.eC = p.f_out;
+  d.oC = p.pitch_out;
+  const int64_t batch = p.M / p.rows;
+  const dim3 grid(static_cast<unsigned>((d.N + kBN - 1) / kBN), static_cast<unsigned>((d.M + kBM - 1) / kBM),
+                  static_cast<unsigned>(batch * outer));
+  gemm_simt<T><<<grid, 256, 0, s>>>(d, in, M, out, run);
   EDAB_LAUNCH("gemm_simt");
 }
 
@@ -315,30 +335,70 @@ struct PlanKey {
   }
 };
 
+// tf32 round-to-nearest (ties away from zero) of a float32, on the host: the hi / lo split of the
+// tensor-core bases (cvt.rna.tf32.f32 rounds the same way).
+float tf32_rna(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
 template <class T>
 void upload_axis(OrientPlan& p, int a, int32_t n) {
   // the bases in long double, rounded once to the dtype
   const long double pi = 3.141592653589793238462643383279502884L;
-  std::vector<T> fwd(static_cast<size_t>(n) * n), ic(static_cast<size_t>(n) * n), is(static_cast<size_t>(n) * n);
+  const size_t nn = static_cast<size_t>(n) * n;
+  std::vector<T> fwd(nn), ic(nn), is(nn);
+  std::vector<long double> exact_c(nn), exact_s(nn);
   for (int32_t k = 0; k < n; ++k) {
     const long double ck = std::sqrt((k ? 2.0L : 1.0L) / static_cast<long double>(n));
     for (int32_t x = 0; x < n; ++x) {
       const int64_t q = (static_cast<int64_t>(k) * (2 * x + 1)) % (4 * static_cast<int64_t>(n));
       const long double ang = pi * static_cast<long double>(q) / static_cast<long double>(2 * n);
-      const T cv = static_cast<T>(ck * std::cos(ang));
-      const T sv = static_cast<T>(ck * std::sin(ang));
-      fwd[static_cast<size_t>(k) * n + x] = cv;
-      ic[static_cast<size_t>(x) * n + k] = cv;
-      is[static_cast<size_t>(x) * n + k] = sv;
+      const long double cv = ck * std::cos(ang), sv = ck * std::sin(ang);
+      exact_c[static_cast<size_t>(k) * n + x] = cv;
+      exact_s[static_cast<size_t>(k) * n + x] = sv;
+      fwd[static_cast<size_t>(k) * n + x] = static_cast<T>(cv);
+      ic[static_cast<size_t>(x) * n + k] = static_cast<T>(cv);
+      is[static_cast<size_t>(x) * n + k] = static_cast<T>(sv);
     }
   }
-  const size_t bytes = sizeof(T) * static_cast<size_t>(n) * n;
+  const size_t bytes = sizeof(T) * nn;
   EDAB_CUDA(cudaMalloc(&p.fwd[a], bytes));
   EDAB_CUDA(cudaMalloc(&p.icos[a], bytes));
   EDAB_CUDA(cudaMalloc(&p.isin[a], bytes));
   EDAB_CUDA(cudaMemcpy(p.fwd[a], fwd.data(), bytes, cudaMemcpyHostToDevice));
   EDAB_CUDA(cudaMemcpy(p.icos[a], ic.data(), bytes, cudaMemcpyHostToDevice));
   EDAB_CUDA(cudaMemcpy(p.isin[a], is.data(), bytes, cudaMemcpyHostToDevice));
+  if constexpr (std::is_same_v<T, float>) {
+    // [2][npad][kpad]: row j holds B(j, k) (hi), row npad + j its lo part
+    const int32_t kpad = static_cast<int32_t>(pad32(n));
+    const int32_t npad = (n + 127) / 128 * 128;
+    p.kpad[a] = kpad;
+    p.npad[a] = npad;
+    const size_t tb = static_cast<size_t>(2) * npad * kpad;
+    auto split = [&](auto&& value, void** dst) {
+      std::vector<float> h(tb, 0.0f);
+      for (int32_t j = 0; j < n; ++j) {
+        for (int32_t k = 0; k < n; ++k) {
+          const long double v = value(j, k);
+          const float hi = tf32_rna(static_cast<float>(v));
+          const float lo = tf32_rna(static_cast<float>(v - static_cast<long double>(hi)));
+          h[static_cast<size_t>(j) * kpad + k] = hi;
+          h[static_cast<size_t>(npad + j) * kpad + k] = lo;
+        }
+      }
+      EDAB_CUDA(cudaMalloc(dst, tb * sizeof(float)));
+      EDAB_CUDA(cudaMemcpy(*dst, h.data(), tb * sizeof(float), cudaMemcpyHostToDevice));
+    };
+    // forward: output frequency j, input sample k; inverse: output sample j, input frequency k
+    split([&](int32_t j, int32_t k) { return exact_c[static_cast<size_t>(j) * n + k]; }, &p.tc_fwd[a]);
+    split([&](int32_t j, int32_t k) { return exact_c[static_cast<size_t>(k) * n + j]; }, &p.tc_icos[a]);
+    split([&](int32_t j, int32_t k) { return exact_s[static_cast<size_t>(k) * n + j]; }, &p.tc_isin[a]);
+  }
 }
 
 }  // namespace
@@ -367,15 +427,63 @@ const OrientPlan& orient_plan(const Geom& g, bool f64) {
 }
 
 template <class T>
+void transform_axes(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* in, T* out, T* buf0, T* buf1,
+                    const int* kinds, const int32_t* run, int32_t* err) {
+  const int D = g.dim;
+  Layout L = element_layout(g);
+  const T* src = in;
+  for (int step = 0; step < D; ++step) {
+    const RotPass p = make_pass(g, L);
+    const int a = L.ax[D - 1];
+    T* dst = step == D - 1 ? out : (src == buf0 ? buf1 : buf0);
+    const int which = kinds[a];
+    if constexpr (std::is_same_v<T, float>) {
+      const void* B = which == 0 ? plan.tc_fwd[a] : (which == 1 ? plan.tc_icos[a] : plan.tc_isin[a]);
+      rot_pass_tc(s, p, static_cast<const float*>(B), plan.kpad[a], plan.npad[a], src, dst, run, err);
+    } else {
+      const void* B = which == 0 ? plan.fwd[a] : (which == 1 ? plan.icos[a] : plan.isin[a]);
+      rot_pass_simt<T>(s, p, g.n[a], static_cast<const T*>(B), src, dst, run);
+    }
+    L = rotated(L);
+    src = dst;
+  }
+}
+template void transform_axes<float>(cudaStream_t, const Geom&, const OrientPlan&, const float*, float*, float*,
+                                    float*, const int*, const int32_t*, int32_t*);
+template void transform_axes<double>(cudaStream_t, const Geom&, const OrientPlan&, const double*, double*, double*,
+                                     double*, const int*, const int32_t*, int32_t*);
+
+int64_t orient_layout_samples(const Geom& g) {
+  Layout L = element_layout(g);
+  int64_t fmax = 0;
+  for (int i = 0; i < g.dim; ++i) {
+    fmax = std::max(fmax, layout_field(g, L));
+    L = rotated(L);
+  }
+  return fmax;
+}
+
+int64_t orient_work_samples(const Geom& g) {
+  const int D = g.dim;
+  return g.batch * (3 * orient_layout_samples(g) + static_cast<int64_t>(D + D * (D + 1) / 2) * g.field);
+}
+
+template <class T>
 void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* r, Elem* el, const int32_t* run,
-                 T* const* n, T* coh, T* work, double two_sigma2) {
+                 T* const* n, T* coh, T* work, double two_sigma2, int32_t* err) {
   const int D = g.dim;
   const int64_t F = g.batch * g.field;
-  T* X = work;           // the band spectrum
-  T* Y = work + F;       // a component spectrum
-  T* Z = work + 2 * F;   // ping-pong buffer of the axis passes
-  T* R1 = work + 3 * F;  // D fields
-  T* R2 = R1 + D * F;    // D (D + 1) / 2 fields
+  const int64_t Fw = g.batch * orient_layout_samples(g);
+  T* X = work;            // the band spectrum
+  T* Y = work + Fw;       // a component spectrum (and a pass buffer)
+  T* Z = work + 2 * Fw;   // pass buffer
+  T* R1 = work + 3 * Fw;  // D fields
+  T* R2 = R1 + D * F;     // D (D + 1) / 2 fields
+  auto transform = [&](const T* in, T* out, auto&& mats) {
+    int kinds[kMaxDim] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) kinds[a] = mats(a);
+    transform_axes<T>(s, g, plan, in, out, Z, Y, kinds, run, err);
+  };
   // mean, then f = r - mean (the difference in double, rounded to T)
   // the means and the chunk sums at the head of Z, consumed before Z is used
   const int64_t nchunks = (g.field + kMeanChunk - 1) / kMeanChunk;
@@ -390,14 +498,8 @@ void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T*
              [=] __device__(int64_t b, int64_t, int64_t i) {
                Y[i] = static_cast<T>(__dsub_rn(static_cast<double>(r[i]), mean[b]));
              });
-  // forward DCT-II along every axis: Y -> X (ping-pong through Z)
-  const T* src = Y;
-  for (int a = 0; a < D; ++a) {
-    T* dst = (a == D - 1) ? X : ((src == Z) ? Y : Z);
-    if (a == D - 1 && src == X) dst = Z;  // (never: src is Y or Z)
-    apply_axis<T>(s, g, a, static_cast<const T*>(plan.fwd[a]), src, dst, run);
-    src = dst;
-  }
+  // forward DCT-II along every axis: Y -> X
+  transform(Y, X, [](int) { return 0; });
   // the band: X *= G(rad), G the one-octave log-Gabor at f0 = 1 / w (G(0) = 0)
   const Geom gg = g;
   for_voxels(s, g, [=] __device__(int64_t b) { return run[b] != 0; },
@@ -440,13 +542,7 @@ void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T*
                      Y[i] = static_cast<T>(__dmul_rn(m, static_cast<double>(X[i])));
                    });
         const int odd = kind == 0 ? (1 << a) : (a == b2 ? 0 : ((1 << a) | (1 << b2)));
-        const T* csrc = Y;
-        for (int ax = 0; ax < D; ++ax) {
-          T* dst = (ax == D - 1) ? out : (csrc == Z ? Y : Z);
-          const void* M = ((odd >> ax) & 1) ? plan.isin[ax] : plan.icos[ax];
-          apply_axis<T>(s, g, ax, static_cast<const T*>(M), csrc, dst, run);
-          csrc = dst;
-        }
+        transform(Y, out, [odd](int ax) { return ((odd >> ax) & 1) ? 2 : 1; });
       }
     }
   }
@@ -457,8 +553,8 @@ void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T*
 }
 
 template void orientation<float>(cudaStream_t, const Geom&, const OrientPlan&, const float*, Elem*, const int32_t*,
-                                 float* const*, float*, float*, double);
+                                 float* const*, float*, float*, double, int32_t*);
 template void orientation<double>(cudaStream_t, const Geom&, const OrientPlan&, const double*, Elem*, const int32_t*,
-                                  double* const*, double*, double*, double);
+                                  double* const*, double*, double*, double, int32_t*);
 
 }  // namespace edab

@@ -24,17 +24,48 @@ struct OrientPlan {
   void* fwd[kMaxDim] = {nullptr, nullptr, nullptr};
   void* icos[kMaxDim] = {nullptr, nullptr, nullptr};
   void* isin[kMaxDim] = {nullptr, nullptr, nullptr};
+  // float32 only, for the tensor cores: the same bases split into tf32 hi and lo parts,
+  // [2][npad][kpad] (hi rows, then lo rows; zero beyond n), kpad = n rounded up to 32, npad to 128
+  void* tc_fwd[kMaxDim] = {nullptr, nullptr, nullptr};
+  void* tc_icos[kMaxDim] = {nullptr, nullptr, nullptr};
+  void* tc_isin[kMaxDim] = {nullptr, nullptr, nullptr};
+  int32_t kpad[kMaxDim] = {0, 0, 0};
+  int32_t npad[kMaxDim] = {0, 0, 0};
 };
 // The plan of a geometry and dtype on the current device (cached for the life of the process).
 const OrientPlan& orient_plan(const Geom& g, bool f64);
-// Work fields of the orientation: the spectrum, the component spectrum, a transpose buffer, R1 (D),
-// R2 (D (D + 1) / 2).
-inline int orient_work_fields(int D) { return 3 + D + D * (D + 1) / 2; }
+// Samples of the orientation's work area: three ping-pong fields large enough for every rotated
+// layout of an element (the spectrum, the component spectrum, a pass buffer), then R1 (D fields) and
+// R2 (D (D + 1) / 2 fields) in the element layout.
+int64_t orient_work_samples(const Geom& g);
+
+// One axis pass of a rotated layout: the layout's contiguous axis (extent K, rows pitch_in apart,
+// `rows` rows per element, element fields f_in apart) is transformed and stored with that axis
+// first and the previous second-fastest axis (extent n_lo, padded to pitch_out) contiguous: row r =
+// hi * n_lo + lo of element b stores column j at b * f_out + j * s_j + hi * pitch_out + lo.
+struct RotPass {
+  int64_t M;  // rows of the batch
+  int32_t K;
+  int64_t pitch_in, rows, f_in, n_lo, pitch_out, s_j, f_out;
+};
+// The pass on the tensor cores (float32, 3xTF32): basis [2][npad][kpad] hi / lo; *err set when a
+// bounded wait of the kernel expired.
+void rot_pass_tc(cudaStream_t s, const RotPass& p, const float* basis, int32_t kpad, int32_t npad, const float* in,
+                 float* out, const int32_t* run, int32_t* err);
+
+// The separable transform of every element with run[b] along all axes (last axis first), kinds[a]
+// = 0 forward DCT-II, 1 inverse cosine, 2 inverse sine basis on axis a: in (element layout) -> out
+// (element layout) through D rotated passes, ping-ponging between buf0 and buf1 (each holding
+// every rotated layout of the batch; in may be buf1, and is then overwritten).
+template <class T>
+void transform_axes(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* in, T* out, T* buf0, T* buf1,
+                    const int* kinds, const int32_t* run, int32_t* err);
+int64_t orient_layout_samples(const Geom& g);  // the largest rotated layout of one element
 
 // n[0..D-1] and coh of every element with run[b]; el[b].w is the band's window; a non-finite
 // tensor sets el[b].nonfinite.
 template <class T>
 void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* r, Elem* el, const int32_t* run,
-                 T* const* n, T* coh, T* work, double two_sigma2);
+                 T* const* n, T* coh, T* work, double two_sigma2, int32_t* err);
 
 }  // namespace edab

@@ -15,8 +15,10 @@ from conftest import ROOT
 
 
 def declared() -> list[str]:
-    text = (ROOT / "include" / "eda_b200.h").read_text()
-    return re.findall(r"EDA_API\s+[\w\s\*]+?\b(eda_\w+)\s*\(", text)
+    names = []
+    for header in sorted((ROOT / "include").glob("*.h")):
+        names += re.findall(r"EDA_API\s+[\w\s\*]+?\b(eda_\w+)\s*\(", header.read_text())
+    return names
 
 
 def test_the_library_exports_every_declared_entry_point():
