@@ -181,7 +181,10 @@ int eda_device_info(int device, char* buf, size_t len) {
 }
 
 int eda_release_workspace(void) {
-  return guarded([&] { edab::thread_workspace().release(); });
+  return guarded([&] {
+    edab::thread_workspace().release();
+    edab::thread_staging().release();
+  });
 }
 
 }  // extern "C"

@@ -84,18 +84,21 @@ __device__ __forceinline__ T fold_identity() {
 struct Win {
   int32_t r, wa, o, k_lo, nseg, cps;
 };
-__device__ __forceinline__ int32_t geom_n(const Geom& g, int a) { return a == 0 ? g.n[0] : (a == 1 ? g.n[1] : g.n[2]); }
-__device__ __forceinline__ int64_t geom_stride(const Geom& g, int a) {
-  return a == 0 ? g.stride[0] : (a == 1 ? g.stride[1] : g.stride[2]);
+// 32-bit arithmetic throughout (n <= 8192 and wa <= 2n - 1, so n (wa + 1) / 2 < 2^27): the 64-bit
+// integer divisions of a general formula are long emulated sequences on the GPU.
+__device__ __forceinline__ int32_t floor_div32(int32_t a, int32_t b) {  // b > 0
+  const int32_t q = a / b;
+  return (a % b != 0 && a < 0) ? q - 1 : q;
 }
 __device__ __forceinline__ Win make_win(int32_t n, int32_t w) {
   Win q;
-  const int32_t half = (w - 1) / 2;
+  const int32_t half = (w - 1) >> 1;
   q.r = min(half, n - 1);
   q.wa = 2 * q.r + 1;
-  q.o = static_cast<int32_t>((static_cast<int64_t>(n) * ((q.wa + 1) / 2)) % q.wa);
-  q.k_lo = static_cast<int32_t>(floor_div(static_cast<int64_t>(q.r) - q.o, q.wa));
-  const int32_t k_hi = static_cast<int32_t>(floor_div(static_cast<int64_t>(n) - 1 + q.r - q.o, q.wa));
+  q.o = static_cast<int32_t>((static_cast<uint32_t>(n) * static_cast<uint32_t>((q.wa + 1) >> 1)) %
+                             static_cast<uint32_t>(q.wa));
+  q.k_lo = floor_div32(q.r - q.o, q.wa);
+  const int32_t k_hi = floor_div32(n - 1 + q.r - q.o, q.wa);
   q.nseg = k_hi - q.k_lo + 1;
   q.cps = (q.wa + 31) >> 5;
   return q;
@@ -185,53 +188,147 @@ __device__ __forceinline__ void chunk_g(const T* __restrict__ vp, T* __restrict_
   }
 }
 
+// The partial folds of a chunk inside the line (fewer than 32 samples, or a chunk that starts
+// before the first output). v: the chunk's first sample (STEP words per sample), r: the output slot
+// of the chunk's first sample (STEP words per sample); only samples i >= skip have an output.
+// Max / min fold from the carry (the operation's identity without one); sums fold locally and add
+// the carry to every output (the canonical G = carry op local).
+template <class T, int OP>
+__device__ __forceinline__ T fold_init(T cv, T v0) {
+  if constexpr (OP == kOpSum) return v0;
+  else return fop<OP>(cv, v0);
+}
+template <class T, int OP>
+__device__ __forceinline__ T fold_out(T cv, T loc) {
+  if constexpr (OP == kOpSum) return add_rn(cv, loc);
+  else return loc;
+}
+template <class T, int OP, int STEP>
+__device__ __forceinline__ T partial_total(const T* __restrict__ v, int32_t len) {
+  T loc = v[0];
+  int32_t i = 1;
+  for (; i + 3 < len; i += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) loc = fop<OP>(loc, v[(i + u) * STEP]);
+  }
+  for (; i < len; ++i) loc = fop<OP>(loc, v[i * STEP]);
+  return loc;
+}
+// H: the output of sample i is stored (slots step back with the samples: STEP = -PP for both)
+template <class T, int OP, int PP>
+__device__ __forceinline__ void partial_h(const T* __restrict__ v, T* __restrict__ r, int32_t len, int32_t skip,
+                                          T cv) {
+  T loc = fold_init<T, OP>(cv, v[0]);
+  if (skip == 0) r[0] = fold_out<T, OP>(cv, loc);
+  int32_t i = 1;
+  const int32_t pre = min(skip, len);
+  for (; i < pre; ++i) loc = fop<OP>(loc, v[-i * PP]);
+  for (; i + 3 < len; i += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      loc = fop<OP>(loc, v[-(i + u) * PP]);
+      r[-(i + u) * PP] = fold_out<T, OP>(cv, loc);
+    }
+  }
+  for (; i < len; ++i) {
+    loc = fop<OP>(loc, v[-i * PP]);
+    r[-i * PP] = fold_out<T, OP>(cv, loc);
+  }
+}
+// G combined with the H in the slots (STEP = +PP); the chunk's last sample, when it ends an aligned
+// box window (aligned_end), takes (H + G) * 0.5.
+template <class T, int OP>
+__device__ __forceinline__ void combine_g(T* __restrict__ slot, T cv, T loc, bool half) {
+  if constexpr (OP == kOpSum) {
+    const T y = add_rn(*slot, add_rn(cv, loc));
+    *slot = half ? mul_rn(y, T(0.5)) : y;
+  } else {
+    *slot = fop<OP>(*slot, loc);
+  }
+}
+template <class T, int OP, int PP>
+__device__ __forceinline__ void partial_g(const T* __restrict__ v, T* __restrict__ r, int32_t len, int32_t skip,
+                                          T cv, bool aligned_end) {
+  const int32_t last = len - 1;
+  T loc = fold_init<T, OP>(cv, v[0]);
+  if (last == 0) {
+    if (skip == 0) combine_g<T, OP>(r, cv, loc, aligned_end);
+    return;
+  }
+  if (skip == 0) combine_g<T, OP>(r, cv, loc, false);
+  int32_t i = 1;
+  const int32_t pre = min(skip, last);
+  for (; i < pre; ++i) loc = fop<OP>(loc, v[i * PP]);
+  for (; i + 3 < last; i += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      loc = fop<OP>(loc, v[(i + u) * PP]);
+      combine_g<T, OP>(r + (i + u) * PP, cv, loc, false);
+    }
+  }
+  for (; i < last; ++i) {
+    loc = fop<OP>(loc, v[i * PP]);
+    combine_g<T, OP>(r + i * PP, cv, loc, false);
+  }
+  loc = fop<OP>(loc, v[last * PP]);
+  if (last >= skip) combine_g<T, OP>(r + last * PP, cv, loc, aligned_end);
+}
+
+// The fold tasks (segment k, chunk c) of one worker, chunk-major (u = c nseg + k, u = first,
+// first + stride, ..): the workers of a warp take the same chunk of consecutive segments (wa
+// samples apart, spreading their shared-memory banks). Advanced without divisions.
+struct Tasks {
+  int32_t k, c, dk, dc;
+  __device__ __forceinline__ Tasks(int32_t first, int32_t stride, int32_t nseg)
+      : k(first % nseg), c(first / nseg), dk(stride % nseg), dc(stride / nseg) {}
+  __device__ __forceinline__ void next(int32_t nseg) {
+    k += dk;
+    c += dc;
+    if (k >= nseg) {
+      k -= nseg;
+      ++c;
+    }
+  }
+};
+
 // One stage on the staged lines of this CTA: V -> R (both n x PP, line p at column p), tot: the
-// chunk totals / carries [2][TS][PP]. Workers: P lanes each (lane % P = the line).
+// chunk totals / carries [2][TS][PP] (slot k cps + c). Workers: P lanes each (lane % P = the line).
 template <class T, int OP, int P>
-__device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int32_t n, int32_t TS,
-                          const Win& q) {
+__device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int32_t n,
+                                          int32_t TS, const Win& q) {
   constexpr int PP = line_pitch(P);
   constexpr int slots = 32 / P;
   constexpr int workers = kWarps * slots;
   const int lane = threadIdx.x & 31;
   const int p = lane & (P - 1);
   const int worker = (threadIdx.x >> 5) * slots + lane / P;
-  const int32_t per_dir = q.nseg * q.cps;
   const int32_t e_max = n - 1 + q.r;
   const T* Vp = V + p;
   T* Rp = R + p;
   const T idn = fold_identity<T, OP>();
-  // Tasks are enumerated chunk-major (u = c nseg + k), so the workers of a warp take the same
-  // chunk of consecutive segments (wa samples apart, spreading their shared-memory banks) rather
-  // than consecutive chunks of one segment (32 samples apart: the same banks). slot = k cps + c.
   if (q.cps > 1) {
-    // phase 1: chunk totals of both directions
-    for (int32_t t = worker; t < 2 * per_dir; t += workers) {
-      const int dir = t >= per_dir;
-      const int32_t u = t - dir * per_dir;
-      const int32_t c = u / q.nseg, k = u - c * q.nseg;
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    // phase 1: chunk totals; half of the workers take the line, half the reversed line
+    constexpr int half = workers / 2;
+    const int dir = worker >= half;
+    for (Tasks t(worker - dir * half, half, q.nseg); t.c < q.cps; t.next(q.nseg)) {
+      const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
-      const int32_t c0 = s + 32 * c;
+      const int32_t c0 = s + 32 * t.c;
       if (c0 > e_last) continue;
       const int32_t c1 = min(c0 + 31, e_last);
       T total;
       if (c0 >= 0 && c1 <= n - 1) {
-        const T* vp = Vp + (dir ? n - 1 - c0 : c0) * PP;
-        if (c1 == c0 + 31) {
-          total = dir ? chunk_total<T, OP, -PP>(vp) : chunk_total<T, OP, PP>(vp);
+        if (dir) {
+          const T* vp = Vp + (n - 1 - c0) * PP;
+          total = c1 == c0 + 31 ? chunk_total<T, OP, -PP>(vp) : partial_total<T, OP, -PP>(vp, c1 - c0 + 1);
         } else {
-          const int32_t step = dir ? -PP : PP;
-          total = *vp;
-          for (int32_t e = c0 + 1; e <= c1; ++e) {
-            vp += step;
-            total = fop<OP>(total, *vp);
-          }
+          const T* vp = Vp + c0 * PP;
+          total = c1 == c0 + 31 ? chunk_total<T, OP, PP>(vp) : partial_total<T, OP, PP>(vp, c1 - c0 + 1);
         }
       } else {
         total = fold_chunk<T, OP>(Vp, PP, n, c0, c1, dir, [](int32_t, T) {});
       }
-      tot[(dir * TS + k * q.cps + c) * PP + p] = total;
+      tot[(dir * TS + t.k * q.cps + t.c) * PP + p] = total;
     }
     __syncthreads();
     // phase 2: exclusive carries per segment, in place (slot c holds the carry of chunk c >= 1)
@@ -252,34 +349,18 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     __syncthreads();
   }
   // phase 3: H (the reversed line's G) into R at the output slots n - 1 + r - e (e >= r)
-  for (int32_t u = worker; u < per_dir; u += workers) {
-    const int32_t c = u / q.nseg, k = u - c * q.nseg;
-    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+  for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
+    const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
-    const int32_t c0 = s + 32 * c;
+    const int32_t c0 = s + 32 * t.c;
     if (c0 > e_last) continue;
     const int32_t c1 = min(c0 + 31, e_last);
-    const T cv = c > 0 ? tot[(TS + k * q.cps + c) * PP + p] : idn;
+    const T cv = t.c > 0 ? tot[(TS + t.k * q.cps + t.c) * PP + p] : idn;
     if (c0 >= 0 && c1 <= n - 1) {
       const T* vp = Vp + (n - 1 - c0) * PP;
-      if (c1 == c0 + 31 && c0 >= q.r) {
-        chunk_h<T, OP, PP>(vp, Rp + (n - 1 + q.r - c0) * PP, cv);
-      } else {
-        // first output at e = max(c0, r); slots step back one sample per sample
-        const int32_t e_out = max(c0, q.r);
-        T* rp = Rp + (n - 1 + q.r - e_out) * PP;
-        T loc = OP == kOpSum ? *vp : fop<OP>(cv, *vp);
-        for (int32_t e = c0; e <= c1; ++e) {
-          if (e > c0) {
-            vp -= PP;
-            loc = fop<OP>(loc, *vp);
-          }
-          if (e >= e_out) {
-            *rp = OP == kOpSum ? add_rn(cv, loc) : loc;
-            rp -= PP;
-          }
-        }
-      }
+      T* rp = Rp + (n - 1 + q.r - c0) * PP;  // the slot of e = c0 (written only when c0 >= r)
+      if (c1 == c0 + 31 && c0 >= q.r) chunk_h<T, OP, PP>(vp, rp, cv);
+      else partial_h<T, OP, PP>(vp, rp, c1 - c0 + 1, max(0, q.r - c0), cv);
     } else {
       fold_chunk<T, OP>(Vp, PP, n, c0, c1, 1, [&](int32_t e, T loc) {
         if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = fop<OP>(cv, loc);
@@ -288,39 +369,19 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   }
   __syncthreads();
   // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r)), slot x = e - r
-  for (int32_t u = worker; u < per_dir; u += workers) {
-    const int32_t c = u / q.nseg, k = u - c * q.nseg;
-    const int32_t s = q.o + (q.k_lo + k) * q.wa;
-    const int32_t e_last = min(s + q.wa - 1, e_max);
-    const int32_t c0 = s + 32 * c;
+  for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
+    const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
+    const int32_t e_al = s + q.wa - 1;
+    const int32_t e_last = min(e_al, e_max);
+    const int32_t c0 = s + 32 * t.c;
     if (c0 > e_last) continue;
     const int32_t c1 = min(c0 + 31, e_last);
-    const T cv = c > 0 ? tot[(k * q.cps + c) * PP + p] : idn;
-    const int32_t e_al = s + q.wa - 1;
+    const T cv = t.c > 0 ? tot[(t.k * q.cps + t.c) * PP + p] : idn;
     if (c0 >= 0 && c1 <= n - 1) {
       const T* vp = Vp + c0 * PP;
-      if (c1 == c0 + 31 && c0 >= q.r) {
-        chunk_g<T, OP, PP>(vp, Rp + (c0 - q.r) * PP, cv, c1 == e_al);
-      } else {
-        const int32_t e_out = max(c0, q.r);
-        T* rp = Rp + (e_out - q.r) * PP;
-        T loc = OP == kOpSum ? *vp : fop<OP>(cv, *vp);
-        for (int32_t e = c0; e <= c1; ++e) {
-          if (e > c0) {
-            vp += PP;
-            loc = fop<OP>(loc, *vp);
-          }
-          if (e >= e_out) {
-            if constexpr (OP == kOpSum) {
-              const T y = add_rn(*rp, add_rn(cv, loc));
-              *rp = e == e_al ? mul_rn(y, T(0.5)) : y;
-            } else {
-              *rp = fop<OP>(*rp, loc);
-            }
-            rp += PP;
-          }
-        }
-      }
+      T* rp = Rp + (c0 - q.r) * PP;  // the slot of e = c0 (written only when c0 >= r)
+      if (c1 == c0 + 31 && c0 >= q.r) chunk_g<T, OP, PP>(vp, rp, cv, c1 == e_al);
+      else partial_g<T, OP, PP>(vp, rp, c1 - c0 + 1, max(0, q.r - c0), cv, c1 == e_al);
     } else {
       fold_chunk<T, OP>(Vp, PP, n, c0, c1, 0, [&](int32_t e, T loc) {
         if (e < q.r) return;
@@ -398,12 +459,13 @@ __global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) 
       ok = row < g.rows;
       base = row * g.pitch;
     } else {
-      const int64_t inner = axis_stride;
-      const int64_t gpo = (inner + P - 1) / P;
-      const int64_t o = grp / gpo;
-      const int64_t c = (grp - o * gpo) * P + p;
-      ok = c < inner && (c % g.pitch) < n_last;
-      base = o * static_cast<int64_t>(n) * inner + c;
+      // 32-bit divisions (an element holds fewer than 2^31 samples)
+      const uint32_t inner = static_cast<uint32_t>(axis_stride);
+      const uint32_t gpo = (inner + P - 1) / P;
+      const uint32_t o = static_cast<uint32_t>(grp) / gpo;
+      const uint32_t c = (static_cast<uint32_t>(grp) - o * gpo) * P + p;
+      ok = c < inner && (c % static_cast<uint32_t>(g.pitch)) < static_cast<uint32_t>(n_last);
+      base = static_cast<int64_t>(o) * n * inner + c;
     }
     base_s[p] = base;
     ok_s[p] = ok ? 1 : 0;

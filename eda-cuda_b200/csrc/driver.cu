@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <cstring>
 #include <mutex>
+#include <thread>
 
 namespace edab {
 
@@ -49,6 +51,74 @@ void Workspace::reserve(size_t bytes) {
 Workspace& thread_workspace() {
   thread_local Workspace ws;
   return ws;
+}
+
+HostStaging::~HostStaging() { release(); }
+
+unsigned char* HostStaging::piece(int i) {
+  if (!base_) {
+    void* p = nullptr;
+    EDAB_CUDA(cudaHostAlloc(&p, 2 * kPiece, cudaHostAllocPortable));
+    base_ = static_cast<unsigned char*>(p);
+  }
+  return base_ + static_cast<size_t>(i) * kPiece;
+}
+
+void HostStaging::release() {
+  if (base_) cudaFreeHost(base_);
+  base_ = nullptr;
+}
+
+HostStaging& thread_staging() {
+  thread_local HostStaging st;
+  return st;
+}
+
+namespace {
+// dst[0, bytes) = src[0, bytes) by up to `threads` host threads
+void parallel_memcpy(unsigned char* dst, const unsigned char* src, size_t bytes, unsigned threads) {
+  const size_t min_share = size_t{1} << 20;
+  const unsigned k = static_cast<unsigned>(std::min<size_t>(threads, std::max<size_t>(1, bytes / min_share)));
+  if (k <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const size_t share = (bytes + k - 1) / k;
+  for (unsigned t = 1; t < k; ++t) {
+    const size_t off = t * share;
+    if (off >= bytes) break;
+    pool.emplace_back([=] { std::memcpy(dst + off, src + off, std::min(share, bytes - off)); });
+  }
+  std::memcpy(dst, src, std::min(share, bytes));
+  for (auto& th : pool) th.join();
+}
+}  // namespace
+
+void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  HostStaging& st = thread_staging();
+  const unsigned threads = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const size_t P = HostStaging::kPiece;
+  const size_t pieces = (bytes + P - 1) / P;
+  cudaEvent_t done[2];
+  EDAB_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+  EDAB_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+  auto issue = [&](size_t i) {
+    const size_t off = i * P, len = std::min(P, bytes - off);
+    EDAB_CUDA(cudaMemcpyAsync(st.piece(static_cast<int>(i & 1)), static_cast<const unsigned char*>(src) + off, len,
+                              cudaMemcpyDeviceToHost, s));
+    EDAB_CUDA(cudaEventRecord(done[i & 1], s));
+  };
+  issue(0);
+  for (size_t i = 0; i < pieces; ++i) {
+    EDAB_CUDA(cudaEventSynchronize(done[i & 1]));
+    if (i + 1 < pieces) issue(i + 1);  // the other piece was copied on in the previous step
+    const size_t off = i * P, len = std::min(P, bytes - off);
+    parallel_memcpy(static_cast<unsigned char*>(dst) + off, st.piece(static_cast<int>(i & 1)), len, threads);
+  }
+  cudaEventDestroy(done[0]);
+  cudaEventDestroy(done[1]);
 }
 
 Run::~Run() {
@@ -101,7 +171,7 @@ void Run::collect(void* dst, bool dst_on_device, cudaStream_t s) {
   }
   EDAB_LAUNCH("collect_kernel");
   if (!dst_on_device) {
-    EDAB_CUDA(cudaMemcpyAsync(dst, out, elems * es, cudaMemcpyDeviceToHost, s));
+    copy_to_pageable(dst, out, elems * es, s);
     EDAB_CUDA(cudaFreeAsync(out, s));
   }
   EDAB_CUDA(cudaFreeAsync(meta, s));

@@ -40,6 +40,25 @@ class Workspace {
 };
 Workspace& thread_workspace();
 
+// Pinned host memory of the calling thread for device-to-host copies into pageable memory: two
+// pieces of kPiece bytes, allocated on first use and kept until released.
+class HostStaging {
+ public:
+  static constexpr size_t kPiece = size_t{32} << 20;
+  ~HostStaging();
+  unsigned char* piece(int i);  // i = 0 or 1
+  void release();
+
+ private:
+  unsigned char* base_ = nullptr;
+};
+HostStaging& thread_staging();
+
+// Copies bytes from device memory src to pageable host memory dst on stream s: the transfers land
+// in the pinned pieces (double-buffered) and host threads copy each piece on while the next one
+// transfers. Returns when dst holds every byte.
+void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 struct Params {
   int32_t max_imf = -1;
   double tie_tolerance = -1.0;  // < 0: 2^-14 (float32) / 2^-30 (float64)

@@ -72,22 +72,56 @@ struct Geom {
   int64_t count;            // unpadded samples per element
   int64_t rows;             // rows of the innermost axis per element
   int32_t n_max;
+  int32_t n_last;            // n[dim - 1] (device code reads this, not n[] at a run-time index)
+  uint64_t pitch_inv;        // ceil(2^64 / pitch): v / pitch = umulhi(v, pitch_inv) for 0 <= v < 2^32
 };
 Geom make_geom(int dim, int64_t batch, const int64_t* n);
 
-__host__ __device__ inline bool is_pad(const Geom& g, int64_t v) { return v % g.pitch >= g.n[g.dim - 1]; }
+// n[a] and stride[a] for a run-time axis a, by selects: a kernel parameter indexed at a run-time
+// index would be copied to local memory.
+__host__ __device__ inline int32_t geom_n(const Geom& g, int a) { return a == 0 ? g.n[0] : (a == 1 ? g.n[1] : g.n[2]); }
+__host__ __device__ inline int64_t geom_stride(const Geom& g, int a) {
+  return a == 0 ? g.stride[0] : (a == 1 ? g.stride[1] : g.stride[2]);
+}
+// The row and column of in-element offset v (0 <= v < 2^32) without a division on the device:
+// umulhi(v, ceil(2^64 / pitch)) is exact since v / 2^64 < 1 / pitch.
+__host__ __device__ inline int64_t pitch_row(const Geom& g, int64_t v) {
+#ifdef __CUDA_ARCH__
+  return static_cast<int64_t>(__umul64hi(static_cast<uint64_t>(v), g.pitch_inv));
+#else
+  return v / g.pitch;
+#endif
+}
+__host__ __device__ inline int64_t pitch_col(const Geom& g, int64_t v) { return v - pitch_row(g, v) * g.pitch; }
+__host__ __device__ inline bool is_pad(const Geom& g, int64_t v) { return pitch_col(g, v) >= g.n_last; }
 __host__ __device__ inline int32_t coord_of(const Geom& g, int64_t v, int a) {
-  if (a == g.dim - 1) return static_cast<int32_t>(v % g.pitch);
-  return static_cast<int32_t>((v / g.stride[a]) % g.n[a]);
+  if (a == g.dim - 1) return static_cast<int32_t>(pitch_col(g, v));
+  return static_cast<int32_t>((v / geom_stride(g, a)) % geom_n(g, a));
 }
 // Coordinates of padded offset v; false for a pad.
 __host__ __device__ inline bool voxel_coords(const Geom& g, int64_t v, int32_t* x) {
-  const int64_t row = v / g.pitch;
+  const int64_t row = pitch_row(g, v);
   const int64_t col = v - row * g.pitch;
-  if (col >= g.n[g.dim - 1]) return false;
+  if (col >= g.n_last) return false;
   x[g.dim - 1] = static_cast<int32_t>(col);
   int64_t q = row;
   for (int a = g.dim - 2; a >= 0; --a) {
+    x[a] = static_cast<int32_t>(q % g.n[a]);
+    q /= g.n[a];
+  }
+  return true;
+}
+
+// voxel_coords for a compile-time D (the Geom parameter and x stay in registers).
+template <int D>
+__device__ __forceinline__ bool voxel_coords_d(const Geom& g, int64_t v, int32_t* x) {
+  const int64_t row = pitch_row(g, v);
+  const int64_t col = v - row * g.pitch;
+  if (col >= g.n[D - 1]) return false;
+  x[D - 1] = static_cast<int32_t>(col);
+  int64_t q = row;
+#pragma unroll
+  for (int a = D - 2; a >= 0; --a) {
     x[a] = static_cast<int32_t>(q % g.n[a]);
     q /= g.n[a];
   }
@@ -255,12 +289,12 @@ inline unsigned blocks_for(int64_t n, int threads = kThreads) {
 // i = b * field + v.
 template <class Run, class F>
 __global__ void __launch_bounds__(kThreads) voxel_kernel(Geom g, Run run, F f) {
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     if (!run(b)) continue;
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-      if (v % g.pitch >= nl) continue;
+      if (pitch_col(g, v) >= nl) continue;
       f(b, v, b * g.field + v);
     }
   }

@@ -53,6 +53,8 @@ Geom make_geom(int dim, int64_t batch, const int64_t* n) {
   g.field = dim == 1 ? g.pitch : static_cast<int64_t>(g.n[0]) * g.stride[0];
   if (g.field > (int64_t{1} << 31)) throw std::invalid_argument("eda: an element's padded field exceeds 2^31 samples");
   g.rows = g.field / g.pitch;
+  g.n_last = g.n[dim - 1];
+  g.pitch_inv = ~uint64_t{0} / static_cast<uint64_t>(g.pitch) + 1;
   return g;
 }
 
@@ -227,10 +229,10 @@ __global__ void __launch_bounds__(kThreads) build_kernel(Geom g, Ctl c, const T*
   __syncthreads();
   const T q = static_cast<T>(c.q), sm1 = static_cast<T>(c.span - 1.0);
   unsigned long long tmin = 0x7ff0000000000000ULL, tmax = 0ULL;
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
        v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (v % g.pitch >= nl) continue;
+    if (pitch_col(g, v) >= nl) continue;
     const int64_t i = b * g.field + v;
     T d, e;
     element_de<T>(L[i], D == 1 ? T(0) : coh[i], q, sm1, &d, &e);
@@ -272,10 +274,10 @@ __global__ void __launch_bounds__(kThreads) weights_kernel(Geom g, Ctl c, const 
   const double w_lo = static_cast<double>(el[b].rung_w[0]);
   const double w_hi = static_cast<double>(el[b].rung_w[K > 0 ? K - 1 : 0]);
   unsigned used = 0u, pts = 0u;
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
        v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (v % g.pitch >= nl) continue;
+    if (pitch_col(g, v) >= nl) continue;
     const int64_t i = b * g.field + v;
     T d, e;
     element_de<T>(L[i], D == 1 ? T(0) : coh[i], q, sm1, &d, &e);
@@ -321,66 +323,67 @@ __global__ void __launch_bounds__(kThreads) weights_kernel(Geom g, Ctl c, const 
 // segment points (D >= 2), at x +- (i / 2) o by D-linear interpolation of the reflected periodic
 // extension. OP 0: max (Dil), 2: max and min (Dil, Ero), 3: box (Avg). The rung cubes of every rung
 // lie in rung0 (rung1: the min cubes) at j * B * field.
-// The four segment points x + (1/2) o, x - (1/2) o, x + o, x - o of a voxel (in this order): per
-// point and axis the offsets (in the element, reflected) of the two interpolation neighbours and
-// their weights. Computed once per voxel and shared by both rungs and both cubes of the gather.
+// Segment point q of a voxel (q = 0..3: x + (1/2) o, x - (1/2) o, x + o, x - o): per axis the
+// offsets (in the element, reflected) of the two interpolation neighbours and their weights.
 template <class T, int D>
-struct SegPoints {
-  int32_t off0[4][D], off1[4][D];
-  T w0[4][D], w1[4][D];
+struct SegPoint {
+  int32_t off0[D], off1[D];
+  T w0[D], w1[D];
 };
 template <class T, int D>
-__device__ __forceinline__ void seg_points(const Geom& g, const int32_t* x, const double* ov, SegPoints<T, D>& P) {
+__device__ __forceinline__ SegPoint<T, D> seg_point(const Geom& g, const int32_t* x, const double* ov, int q) {
+  SegPoint<T, D> P;
+  const double s = static_cast<double>(q / 2 + 1) / 2.0;
+  const int sg = q & 1;
 #pragma unroll
-  for (int i = 1; i <= 2; ++i) {
-    const double s = static_cast<double>(i) / 2.0;
-#pragma unroll
-    for (int sg = 0; sg < 2; ++sg) {
-      const int q = 2 * (i - 1) + sg;
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        const double off = __dmul_rn(s, ov[a]);
-        const double xa = static_cast<double>(x[a]);
-        const double y = sg == 0 ? __dadd_rn(xa, off) : __dsub_rn(xa, off);
-        const double fl = floor(y);
-        const double tt = __dsub_rn(y, fl);
-        const int64_t i0 = static_cast<int64_t>(fl);
-        const T t1 = static_cast<T>(tt);
-        P.w1[q][a] = t1;
-        P.w0[q][a] = sub_rn(T(1), t1);
-        const int64_t st = a == g.dim - 1 ? 1 : g.stride[a];
-        P.off0[q][a] = static_cast<int32_t>(reflect_any(i0, g.n[a]) * st);
-        P.off1[q][a] = static_cast<int32_t>(reflect_any(i0 + 1, g.n[a]) * st);
-      }
-    }
+  for (int a = 0; a < D; ++a) {
+    const double off = __dmul_rn(s, ov[a]);
+    const double xa = static_cast<double>(x[a]);
+    const double y = sg == 0 ? __dadd_rn(xa, off) : __dsub_rn(xa, off);
+    const double fl = floor(y);
+    const double tt = __dsub_rn(y, fl);
+    const int64_t i0 = static_cast<int64_t>(fl);
+    const T t1 = static_cast<T>(tt);
+    P.w1[a] = t1;
+    P.w0[a] = sub_rn(T(1), t1);
+    const int64_t st = a == D - 1 ? 1 : g.stride[a];
+    P.off0[a] = static_cast<int32_t>(reflect_any(i0, g.n[a]) * st);
+    P.off1[a] = static_cast<int32_t>(reflect_any(i0 + 1, g.n[a]) * st);
   }
+  return P;
 }
-// The D-linear interpolation of f at point q: corners in binary order (axis 0 the high bit), each
-// corner's value times its axis weights in axis order, summed in corner order.
+// The D-linear interpolation of f at a segment point: corners in binary order (axis 0 the high
+// bit), each corner's value times its axis weights in axis order, summed in corner order.
 template <class T, int D>
-__device__ __forceinline__ T interp_read(const T* __restrict__ f, const SegPoints<T, D>& P, int q) {
+__device__ __forceinline__ T interp_read(const T* __restrict__ f, const SegPoint<T, D>& P) {
   T acc = T(0);
 #pragma unroll
   for (int corner = 0; corner < (1 << D); ++corner) {
     int32_t off = 0;
 #pragma unroll
-    for (int a = 0; a < D; ++a) off += ((corner >> (D - 1 - a)) & 1) ? P.off1[q][a] : P.off0[q][a];
+    for (int a = 0; a < D; ++a) off += ((corner >> (D - 1 - a)) & 1) ? P.off1[a] : P.off0[a];
     T term = __ldg(f + off);
 #pragma unroll
-    for (int a = 0; a < D; ++a) term = mul_rn(term, ((corner >> (D - 1 - a)) & 1) ? P.w1[q][a] : P.w0[q][a]);
+    for (int a = 0; a < D; ++a) term = mul_rn(term, ((corner >> (D - 1 - a)) & 1) ? P.w1[a] : P.w0[a]);
     acc = add_rn(acc, term);
   }
   return acc;
 }
+template <int OP, class T>
+__device__ __forceinline__ T gather_op(T acc, T v, bool second) {
+  if constexpr (OP == 3) return add_rn(acc, v);
+  else if constexpr (OP == 2) return second ? min_c(acc, v) : max_c(acc, v);
+  else return max_c(acc, v);
+}
 
 template <class T, int D, int OP>
-__global__ void __launch_bounds__(kThreads) gather_kernel(Geom g, const Elem* __restrict__ el,
+__global__ void __launch_bounds__(kThreads, 4) gather_kernel(Geom g, const Elem* __restrict__ el,
                                                          const int32_t* __restrict__ run, const uint8_t* __restrict__ lo,
                                                          const T* __restrict__ t, const T* __restrict__ o0,
                                                          const T* __restrict__ o1, const T* __restrict__ o2,
                                                          const T* __restrict__ rung0, const T* __restrict__ rung1,
                                                          T* __restrict__ out0, T* __restrict__ out1) {
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   const int64_t fe = g.batch * g.field;
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     if (!run[b]) continue;
@@ -388,53 +391,62 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Geom g, const Elem* __
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       int32_t x[kMaxDim];
-      if (!voxel_coords(g, v, x)) continue;
+      if (!voxel_coords_d<D>(g, v, x)) continue;
       (void)nl;
       const int64_t at = b * g.field + v;
       const int l = __ldg(lo + at);
       const T tt = __ldg(t + at);
       const T wl = sub_rn(T(1), tt);
-      T r0 = T(0), r1 = T(0);
-      SegPoints<T, (D >= 2 ? D : 1)> P;
-      bool have_pts = false;
-      for (int side = 0; side < 2; ++side) {
-        const int j = l + side;
-        const T wgt = side == 0 ? wl : tt;
-        if (!(wgt > T(0))) continue;
-        const T* f0 = rung0 + static_cast<int64_t>(j) * fe + b * g.field;
-        const T* f1 = OP == 2 ? rung1 + static_cast<int64_t>(j) * fe + b * g.field : nullptr;
-        T acc0 = __ldg(f0 + v);
-        T acc1 = OP == 2 ? __ldg(f1 + v) : T(0);
-        if constexpr (D >= 2) {
-          if ((pts_mask >> j) & 1u) {
-            if (!have_pts) {
-              double ov[D];
-              ov[0] = static_cast<double>(__ldg(o0 + at));
-              ov[1] = static_cast<double>(__ldg(o1 + at));
-              if constexpr (D >= 3) ov[2] = static_cast<double>(__ldg(o2 + at));
-              seg_points<T, D>(g, x, ov, P);
-              have_pts = true;
+      // side 0: rung l with weight 1 - t, side 1: rung l + 1 with weight t (read only when weighted);
+      // accumulators a<side><cube>: the value at x, then the segment points in order
+      const bool use0 = wl > T(0), use1 = tt > T(0);
+      const T* fa0 = rung0 + static_cast<int64_t>(l) * fe + b * g.field;
+      const T* fb0 = fa0 + fe;
+      const T* fa1 = OP == 2 ? rung1 + static_cast<int64_t>(l) * fe + b * g.field : nullptr;
+      const T* fb1 = OP == 2 ? fa1 + fe : nullptr;
+      T a00 = use0 ? __ldg(fa0 + v) : T(0), a10 = use1 ? __ldg(fb0 + v) : T(0);
+      T a01 = T(0), a11 = T(0);
+      if constexpr (OP == 2) {
+        a01 = use0 ? __ldg(fa1 + v) : T(0);
+        a11 = use1 ? __ldg(fb1 + v) : T(0);
+      }
+      if constexpr (D >= 2) {
+        const bool pts0 = use0 && ((pts_mask >> l) & 1u);
+        const bool pts1 = use1 && ((pts_mask >> (l + 1)) & 1u);
+        if (pts0 || pts1) {
+          double ov[D];
+          ov[0] = static_cast<double>(__ldg(o0 + at));
+          ov[1] = static_cast<double>(__ldg(o1 + at));
+          if constexpr (D >= 3) ov[2] = static_cast<double>(__ldg(o2 + at));
+#pragma unroll 1
+          for (int q = 0; q < 4; ++q) {
+            const SegPoint<T, D> P = seg_point<T, D>(g, x, ov, q);
+            if (pts0) {
+              a00 = gather_op<OP>(a00, interp_read<T, D>(fa0, P), false);
+              if constexpr (OP == 2) a01 = gather_op<OP>(a01, interp_read<T, D>(fa1, P), true);
             }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              if constexpr (OP == 2) {
-                acc0 = max_c(acc0, interp_read<T, D>(f0, P, q));
-                acc1 = min_c(acc1, interp_read<T, D>(f1, P, q));
-              } else if constexpr (OP == 0) {
-                acc0 = max_c(acc0, interp_read<T, D>(f0, P, q));
-              } else {
-                acc0 = add_rn(acc0, interp_read<T, D>(f0, P, q));
-              }
+            if (pts1) {
+              a10 = gather_op<OP>(a10, interp_read<T, D>(fb0, P), false);
+              if constexpr (OP == 2) a11 = gather_op<OP>(a11, interp_read<T, D>(fb1, P), true);
             }
-            if constexpr (OP == 3) acc0 = div_rn(acc0, T(5));
+          }
+          if constexpr (OP == 3) {
+            if (pts0) a00 = div_rn(a00, T(5));
+            if (pts1) a10 = div_rn(a10, T(5));
           }
         }
-        const T v0 = mul_rn(wgt, acc0);
-        const bool add = side == 1 && wl > T(0);
-        r0 = add ? add_rn(r0, v0) : v0;
+      }
+      T r0 = T(0), r1 = T(0);
+      if (use0) {
+        r0 = mul_rn(wl, a00);
+        if constexpr (OP == 2) r1 = mul_rn(wl, a01);
+      }
+      if (use1) {
+        const T v0 = mul_rn(tt, a10);
+        r0 = use0 ? add_rn(r0, v0) : v0;
         if constexpr (OP == 2) {
-          const T v1 = mul_rn(wgt, acc1);
-          r1 = add ? add_rn(r1, v1) : v1;
+          const T v1 = mul_rn(tt, a11);
+          r1 = use0 ? add_rn(r1, v1) : v1;
         }
       }
       out0[at] = r0;
@@ -447,14 +459,14 @@ template <class T, int D>
 __global__ void __launch_bounds__(kThreads) sift_step_kernel(Geom g, int32_t j, Elem* el, const T* __restrict__ r,
                                                             const T* __restrict__ h, const T* __restrict__ mh,
                                                             const T* __restrict__ a, T* __restrict__ hn) {
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     const Elem& e = el[b];
     if (e.status != kActive || !e.sifting) continue;
     uint64_t m_res = 0, m_h = 0;
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-      if (v % g.pitch >= nl) continue;
+      if (pitch_col(g, v) >= nl) continue;
       const int64_t i = b * g.field + v;
       T m = mh[i];
       if (j >= 1) m = mul_rn(a[i], m);
@@ -1259,10 +1271,10 @@ bool Engine<T>::commit() {
   T* r = r_;
   const T* h = h_;
   const Geom g = g_;
-  const int32_t nl = g_.n[g_.dim - 1];
+  const int32_t nl = g_.n_last;
   for_voxels(s_, g_, [=] __device__(int64_t b) { return el[b].status == kActive; },
              [=] __device__(int64_t b, int64_t v, int64_t i) {
-               const int64_t q = v / g.pitch;
+               const int64_t q = pitch_row(g, v);
                const int64_t t = v - q * g.pitch;
                const T hv = h[i];
                rows[(b * c.rows_cap + el[b].n_imfs) * g.count + q * nl + t] = hv;
@@ -1329,11 +1341,11 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
   int32_t* maskp = mask_;
   T* r = r_;
   // start (cpp/src/method/driver.cpp:393-420): the padded copy, the prescale by 2^-ilogb(max|x|)
-  const int32_t nl = g_.n[g_.dim - 1];
+  const int32_t nl = g_.n_last;
   for_samples(s_, B_ * g_.field, [=] __device__(int64_t i) {
     const int64_t b = i / g.field;
     const int64_t v = i - b * g.field;
-    const int64_t q = v / g.pitch;
+    const int64_t q = pitch_row(g, v);
     const int64_t t = v - q * g.pitch;
     r[i] = t < nl ? x[b * g.count + q * nl + t] : T(0);
   });
@@ -1535,11 +1547,11 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
   }
   // finish: the residue row, the rows scaled back
   {
-    const int32_t nl2 = g_.n[g_.dim - 1];
+    const int32_t nl2 = g_.n_last;
     T* rows = rows_;
     for_voxels(s_, g_, [=] __device__(int64_t b) { return el[b].status != kError; },
                [=] __device__(int64_t b, int64_t v, int64_t i) {
-                 const int64_t q = v / g.pitch;
+                 const int64_t q = pitch_row(g, v);
                  const int64_t t = v - q * g.pitch;
                  rows[(b * c.rows_cap + el[b].n_imfs) * g.count + q * nl2 + t] = r[i];
                });

@@ -165,13 +165,13 @@ __global__ void __launch_bounds__(256) mean_partial(Geom g, const T* __restrict_
                                                     int64_t nchunks) {
   __shared__ double sh[256];
   const int64_t b = blockIdx.y, c = blockIdx.x;
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   double acc = 0.0;
   if (run[b]) {
     const T* rb = r + b * g.field;
     const int64_t v1 = min(g.field, (c + 1) * kMeanChunk);
     for (int64_t v = c * kMeanChunk + threadIdx.x; v < v1; v += 256) {
-      if (v % g.pitch < nl) acc = __dadd_rn(acc, static_cast<double>(rb[v]));
+      if (pitch_col(g, v) < nl) acc = __dadd_rn(acc, static_cast<double>(rb[v]));
     }
   }
   sh[threadIdx.x] = acc;
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(256) tensor_eigen(Geom g, const int32_t* run, 
     if (!run[b]) continue;
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-      if (v % g.pitch >= nl) continue;
+      if (pitch_col(g, v) >= nl) continue;
       const int64_t i = b * g.field + v;
       T R1[D], R2[K];
 #pragma unroll

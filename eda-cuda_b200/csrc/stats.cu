@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(kThreads) row_partials(const T* __restrict__ f
                                                          uint64_t* nonfinite) {
   const int lane = threadIdx.x & 31;
   const int64_t total = g.batch * g.rows;
-  const int32_t n = g.n[g.dim - 1];
+  const int32_t n = g.n_last;
   const int32_t nchunks = (n + 31) >> 5;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
   for (int64_t q = blockIdx.x * static_cast<int64_t>(kThreads / 32) + (threadIdx.x >> 5); q < total; q += warps) {
@@ -199,10 +199,10 @@ __device__ __forceinline__ bool sel_item(const Geom& g, const SelView<T>& a, int
   } else {
     const int64_t k = t / g.field;
     const int64_t v = t - k * g.field;
-    const int axis = a.ax[k];
-    if (is_pad(g, v) || coord_of(g, v, axis) >= g.n[axis] - 1) return false;
+    const int axis = k == 0 ? a.ax[0] : (k == 1 ? a.ax[1] : a.ax[2]);
+    if (is_pad(g, v) || coord_of(g, v, axis) >= geom_n(g, axis) - 1) return false;
     const int64_t i = b * g.field + v;
-    const int64_t st = axis == g.dim - 1 ? 1 : g.stride[axis];
+    const int64_t st = axis == g.dim - 1 ? 1 : geom_stride(g, axis);
     val = static_cast<double>(sub_rn(a.sel.field[i + st], a.sel.field[i]));
   }
   if (a.sel.center != nullptr) val = fabs(__dsub_rn(val, a.sel.center[b]));
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
-  const int32_t n = g.n[axis];
+  const int32_t n = geom_n(g, axis);
   const bool contig = axis == g.dim - 1;
   const int32_t nb = (n + kBlk - 1) / kBlk;
   T* X = reinterpret_cast<T*>(smem_raw);      // P x n
@@ -523,18 +523,18 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
       ok = row < g.rows;
       base = row * g.pitch;
     } else {
-      const int64_t inner = g.stride[axis];
+      const int64_t inner = geom_stride(g, axis);
       const int64_t gpo = (inner + P - 1) / P;
       const int64_t o = grp / gpo;
       const int64_t c = (grp - o * gpo) * P + p;
-      ok = c < inner && (c % g.pitch) < g.n[g.dim - 1];
+      ok = c < inner && (c % g.pitch) < g.n_last;
       base = o * static_cast<int64_t>(n) * inner + c;
     }
     base_s[p] = base;
     ok_s[p] = ok ? 1 : 0;
   }
   if (threadIdx.x == 0) count_s = 0;
-  const int64_t step = contig ? 1 : g.stride[axis];
+  const int64_t step = contig ? 1 : geom_stride(g, axis);
   const int64_t eoff = b * g.field;
   __syncthreads();
   const int32_t total = P * n;
@@ -704,8 +704,8 @@ void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32
     const int32_t v = static_cast<int32_t>(i - b * g.field);
     if (L[v] < 0) return;
     for (int a = 0; a < g.dim; ++a) {
-      if (coord_of(g, v, a) + 1 >= g.n[a]) continue;
-      const int32_t u = v + static_cast<int32_t>(a == g.dim - 1 ? 1 : g.stride[a]);
+      if (coord_of(g, v, a) + 1 >= geom_n(g, a)) continue;
+      const int32_t u = v + static_cast<int32_t>(a == g.dim - 1 ? 1 : geom_stride(g, a));
       if (L[u] < 0) continue;
       unite(L, v, u);
     }

@@ -25,13 +25,13 @@ __global__ void to_padded(Geom g, const T* __restrict__ x, T* __restrict__ f) {
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t b = i / g.field, v = i - b * g.field;
     const int64_t col = v % g.pitch, row = v / g.pitch;
-    const int32_t nl = g.n[g.dim - 1];
+    const int32_t nl = g.n_last;
     f[i] = col < nl ? x[b * g.count + row * nl + col] : T(0);
   }
 }
 template <class T>
 __global__ void to_dense(Geom g, int64_t blocks, const T* __restrict__ f, T* __restrict__ y) {
-  const int32_t nl = g.n[g.dim - 1];
+  const int32_t nl = g.n_last;
   const int64_t total = blocks * g.count;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {

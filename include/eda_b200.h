@@ -92,8 +92,8 @@ EDA_API int eda_device_count(void);
 EDA_API int eda_build_info(char* buf, size_t len);
 EDA_API int eda_device_info(int device, char* buf, size_t len);
 
-/* Frees the calling thread's device workspace (the reference's Context::release_unused_memory,
- * cpp/src/runtime/context.cpp:154-160). */
+/* Frees the calling thread's device workspace and its pinned host staging of device-to-host copies
+ * (the reference's Context::release_unused_memory, cpp/src/runtime/context.cpp:154-160). */
 EDA_API int eda_release_workspace(void);
 
 /* The allocation-free decomposition (no counterpart in the reference), for callers that must not
