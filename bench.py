@@ -187,7 +187,8 @@ def run_ours(args) -> None:
     lib = _native.core()._lib
     lib.eda_profile_read.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
-    x_host = workload(BATCH, 1000 + rank)
+    batch = args.batch
+    x_host = workload(batch, 1000 + rank)
     x_dev = torch.from_numpy(x_host).to(dev)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MiB > L2
     stream = torch.cuda.current_stream(dev)
@@ -223,7 +224,7 @@ def run_ours(args) -> None:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = BATCH * world * args.steps / (total_ms / 1000.0)
+    value = batch * world * args.steps / (total_ms / 1000.0)
     # end to end: host input from pinned memory, rows back to the host, every step
     pinned = torch.empty(x_host.shape, dtype=torch.float32).pin_memory()
     pinned.numpy()[...] = x_host
@@ -244,13 +245,13 @@ def run_ours(args) -> None:
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e = BATCH * world * args.steps / (e2e_total / 1000.0)
+    e2e = batch * world * args.steps / (e2e_total / 1000.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = max(1, min(host_cores(), BATCH))
+        threads = max(1, min(host_cores(), batch))
         secs = cpu_oracle(x_host[:threads], threads)
         cpu = {"value": threads / secs, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{threads} of the {BATCH} images ({SIDE}x{SIDE} float32), one per host thread, "
+               "sample": f"{threads} of the {batch} images ({SIDE}x{SIDE} float32), one per host thread, "
                          f"{secs:.1f} s"}
     if pg is not None:
         pg.barrier()
@@ -266,17 +267,125 @@ def run_ours(args) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"2-D {BATCH} x {SIDE}x{SIDE} float32 images per GPU (rings, wavy stripes, blobs, "
+        "config": {"workload": f"2-D {batch} x {SIDE}x{SIDE} float32 images per GPU (rings, wavy stripes, blobs, "
                                "noise), sifts 3", "l2": "flushed between steps (256 MiB write)",
                    "rows_per_element": int(P), "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "cube_pass", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                      "traffic": traffic, "launches": int(cl.value),
+                     "algorithmic_bytes_per_launch": (cb.value / cl.value) if cl.value else None,
                      "share_of_step": (cms.value / total_ms) if total_ms else None},
         "gpu_launches": int(launches.value),
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def other_workload(name: str, seed: int):
+    """The other configurations of the method's benchmark suite (seeded synthetic stand-ins):
+    returns (description, list of fields or one batch array, axes, elements)."""
+    rng = np.random.default_rng(seed)
+    if name == "1d":
+        t = np.arange(2048, dtype=np.float64)
+        x = np.sin(2 * np.pi * t / 8) + 2 * np.sin(2 * np.pi * t / 64) + 3 * np.sin(2 * np.pi * t / 512)
+        x = (x + 0.01 * rng.standard_normal(t.size)).astype(np.float32)[None]
+        return "1-D 1 x 2048 float32 (three tones and noise), sifts 3", x, (1,), 1
+    if name == "3d":
+        n = 256
+        z, y, x = np.mgrid[0:n, 0:n, 0:n].astype(np.float32)
+        out = np.empty((4, n, n, n), np.float32)
+        period = 32 + 32 * z / (n - 1)
+        for b in range(4):
+            c = rng.uniform(0, n, 3)
+            r = np.sqrt((z - c[0]) ** 2 + (y - c[1]) ** 2 + (x - c[2]) ** 2)
+            g = rng.uniform(0, n, 3)
+            f = np.cos(2 * np.pi * r / 8) + np.cos(2 * np.pi * z / period)
+            f += 3 * np.exp(-((z - g[0]) ** 2 + (y - g[1]) ** 2 + (x - g[2]) ** 2) / (2 * 90.0 ** 2))
+            out[b] = f + 0.01 * rng.standard_normal((n, n, n)).astype(np.float32)
+        return "3-D 4 x 256^3 float32 (spherical waves, chirped plane wave, trend, noise), sifts 3", out, (1, 2, 3), 4
+    if name == "ragged1d":
+        xs = []
+        for _ in range(1024):
+            n = int(np.exp(rng.uniform(np.log(256), np.log(8192))))
+            t = np.arange(n, dtype=np.float64)
+            w = rng.uniform(0.05, 0.3)
+            f = np.cos(2 * np.pi * (0.002 * t + 0.5 * (0.2 - 0.002) / n * t * t)) + 0.8 * np.cos(w * t + 0.8 * np.sin(w * t))
+            f += rng.uniform(-1e-3, 1e-3) * t + 0.01 * rng.standard_normal(n)
+            xs.append(f.astype(np.float32))
+        return ("1-D ragged 1024 signals, lengths exp(U[ln 256, ln 8192]) float32 (chirp, FM tone, slope, noise), "
+                "sifts 3", xs, None, 1024)
+    if name == "ragged2d":
+        xs = []
+        for _ in range(256):
+            h, w = (int(v) for v in rng.integers(64, 2049, 2))
+            s = np.sqrt(h * w) / 512
+            y, x = np.mgrid[0:h, 0:w].astype(np.float32)
+            cy, cx = rng.uniform(0, h), rng.uniform(0, w)
+            f = np.cos(2 * np.pi * np.hypot(y - cy, x - cx) / (6 * s))
+            f += 1.5 * np.cos(2 * np.pi * (x + 4 * s * np.sin(2 * np.pi * y / (128 * s))) / (24 * s))
+            for _ in range(2):
+                by, bx = rng.uniform(0, h), rng.uniform(0, w)
+                f += 3 * np.exp(-((y - by) ** 2 + (x - bx) ** 2) / (2 * (80 * s) ** 2))
+            xs.append((f + 0.02 * rng.standard_normal((h, w))).astype(np.float32))
+        return ("2-D ragged 256 images, sides U[64, 2048] float32 (the 2-D recipe scaled by side / 512), sifts 3",
+                xs, None, 256)
+    raise ValueError(name)
+
+
+def run_other(args) -> None:
+    """One JSON line for a configuration other than the 2-D benchmark (1 GPU): decompositions/s with
+    device-resident inputs (CUDA events around each call) and through host inputs (e2e)."""
+    import torch
+
+    import eda
+
+    dev = torch.device("cuda", 0)
+    desc, data, axes, elements = other_workload(args.workload, 2024)
+    ragged = axes is None
+    if ragged:
+        on_dev = [torch.from_numpy(x).to(dev) for x in data]
+        call_dev = lambda: eda.decompose_ragged(on_dev)  # noqa: E731
+        call_host = lambda: eda.decompose_ragged(data)  # noqa: E731
+        h2d = sum(x.nbytes for x in data)
+    else:
+        on_dev = torch.from_numpy(data).to(dev)
+        call_dev = lambda: eda.decompose(on_dev, axes=axes)  # noqa: E731
+        call_host = lambda: eda.decompose(data, axes=axes)  # noqa: E731
+        h2d = data.nbytes
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        call_dev()
+    torch.cuda.synchronize(dev)
+    ms = []
+    with Clocks(0) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            call_dev()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    for _ in range(args.warmup):
+        call_host()
+    wall, d2h = [], 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        out = call_host()
+        wall.append(1000 * (time.perf_counter() - t0))
+        d2h = sum(np.asarray(r).nbytes for r in out) if ragged else out.nbytes
+    total = sum(ms)
+    line = {
+        "metric": f"decompositions/s ({args.workload})", "value": elements * args.steps / (total / 1000.0),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "l2": "flushed between steps (256 MiB write)"},
+        "e2e": {"value": elements * args.steps / (sum(wall) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
 
@@ -292,9 +401,15 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling runs)")
+    ap.add_argument("--batch", type=int, default=BATCH,
+                    help="images per GPU of the 2-D benchmark (64; smaller only for profiling captures)")
+    ap.add_argument("--workload", default="2d", choices=("2d", "1d", "3d", "ragged1d", "ragged2d"),
+                    help="2d: the benchmark (default); the others measure the remaining configurations on 1 GPU")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "2d":
+        run_other(args)
     else:
         run_ours(args)
 

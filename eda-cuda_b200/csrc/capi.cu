@@ -10,6 +10,9 @@
 struct eda_run {
   std::unique_ptr<edab::Run> run;
 };
+struct eda_ragged_run {
+  std::unique_ptr<edab::RaggedRun> run;
+};
 
 namespace {
 
@@ -69,11 +72,70 @@ int eda_decompose(const void* x, int x_on_device, int dtype, int dim, int64_t ba
     p.sifts = params->sifts;
     p.check_finite = params->check_finite != 0;
     p.max_chunk = params->max_chunk;
+    p.orientation = params->orientation != 0;
     auto r = std::make_unique<eda_run>();
     r->run = edab::decompose(x, x_on_device != 0, dtype, dim, batch, n, p, static_cast<cudaStream_t>(stream));
     *out = r.release();
   });
 }
+
+int eda_decompose_ragged(const void* const* x, int x_on_device, int dtype, int dim, int64_t count, const int64_t* n,
+                         const eda_params* params, int32_t workers, void* stream, eda_ragged_run** out) {
+  return guarded([&] {
+    if (!out || !params) throw std::invalid_argument("eda: null argument");
+    edab::Params p;
+    p.max_imf = params->max_imf;
+    p.tie_tolerance = params->tie_tolerance;
+    p.sifts = params->sifts;
+    p.check_finite = params->check_finite != 0;
+    p.max_chunk = params->max_chunk;
+    p.orientation = params->orientation != 0;
+    auto r = std::make_unique<eda_ragged_run>();
+    r->run = edab::decompose_ragged(x, x_on_device != 0, dtype, dim, count, n, p, workers,
+                                    static_cast<cudaStream_t>(stream));
+    *out = r.release();
+  });
+}
+
+int eda_ragged_element(const eda_ragged_run* run, int64_t i, int32_t* rows, int32_t* n_imfs, int32_t* error,
+                       int32_t* windows, int32_t* sifts, double* spacing, double* energy) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("eda: null run");
+    const edab::RaggedRun& R = *run->run;
+    if (i < 0 || i >= static_cast<int64_t>(R.group.size())) throw std::invalid_argument("eda: element index out of range");
+    const edab::Run& r = *R.groups[static_cast<size_t>(R.group[static_cast<size_t>(i)])];
+    const int64_t j = R.index[static_cast<size_t>(i)];
+    const size_t cap1 = static_cast<size_t>(r.rows_cap > 0 ? r.rows_cap - 1 : 0);
+    const int32_t err = r.error[static_cast<size_t>(j)];
+    const int32_t k = err ? 0 : r.n_imfs[static_cast<size_t>(j)];
+    if (rows) *rows = r.rows_of(j);
+    if (n_imfs) *n_imfs = r.n_imfs[static_cast<size_t>(j)];
+    if (error) *error = err;
+    for (int32_t m = 0; m < k; ++m) {
+      const size_t at = static_cast<size_t>(j) * cap1 + static_cast<size_t>(m);
+      if (windows) windows[m] = r.hist_scale[at];
+      if (sifts) sifts[m] = r.hist_sifts[at];
+      if (spacing) spacing[m] = r.hist_spacing[at];
+      if (energy) energy[m] = r.hist_energy[at];
+    }
+  });
+}
+
+int eda_ragged_collect(eda_ragged_run* run, int64_t i, void* dst, int dst_on_device, void* stream) {
+  return guarded([&] {
+    if (!run || !dst) throw std::invalid_argument("eda: null argument");
+    edab::RaggedRun& R = *run->run;
+    if (i < 0 || i >= static_cast<int64_t>(R.group.size())) throw std::invalid_argument("eda: element index out of range");
+    edab::Run& r = *R.groups[static_cast<size_t>(R.group[static_cast<size_t>(i)])];
+    int prev = 0;
+    EDAB_CUDA(cudaGetDevice(&prev));
+    if (prev != r.device) EDAB_CUDA(cudaSetDevice(r.device));
+    r.collect_one(R.index[static_cast<size_t>(i)], dst, dst_on_device != 0, static_cast<cudaStream_t>(stream));
+    if (prev != r.device) EDAB_CUDA(cudaSetDevice(prev));
+  });
+}
+
+void eda_ragged_free(eda_ragged_run* run) { delete run; }
 
 int eda_run_shape(const eda_run* run, int64_t* batch, int32_t* rows, int32_t* K, int64_t* count, int64_t* chunk) {
   return guarded([&] {
@@ -118,6 +180,28 @@ int eda_run_collect(eda_run* run, void* dst, int dst_on_device, void* stream) {
     if (prev != r.device) EDAB_CUDA(cudaSetDevice(r.device));
     r.collect(dst, dst_on_device != 0, static_cast<cudaStream_t>(stream));
     if (prev != r.device) EDAB_CUDA(cudaSetDevice(prev));
+  });
+}
+
+int eda_run_collect_orientation(eda_run* run, void* dir, void* coh, int dst_on_device, void* stream) {
+  return guarded([&] {
+    if (!run || !dir || !coh) throw std::invalid_argument("eda: null argument");
+    edab::Run& r = *run->run;
+    int prev = 0;
+    EDAB_CUDA(cudaGetDevice(&prev));
+    if (prev != r.device) EDAB_CUDA(cudaSetDevice(r.device));
+    r.collect_orientation(dir, coh, dst_on_device != 0, static_cast<cudaStream_t>(stream));
+    if (prev != r.device) EDAB_CUDA(cudaSetDevice(prev));
+  });
+}
+
+int eda_monogenic(const void* x, int x_on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                  int64_t max_chunk, void* out, int out_on_device, int32_t* nonfinite, void* stream) {
+  return guarded([&] {
+    if (!n || !nonfinite || (batch > 0 && (!x || !out))) throw std::invalid_argument("eda: null argument");
+    if (batch == 0) return;
+    edab::monogenic(x, x_on_device != 0, dtype, dim, batch, n, max_chunk, out, out_on_device != 0, nonfinite,
+                    static_cast<cudaStream_t>(stream));
   });
 }
 

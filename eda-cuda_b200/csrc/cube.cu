@@ -432,7 +432,7 @@ struct LineRoles {
 };
 
 template <class T, int P>
-__global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, 5) cube_pass(Geom g, PassArgs<T> a) {
   constexpr int PP = line_pitch(P);
   using Roles = LineRoles<P>;
   extern __shared__ __align__(16) unsigned char smem_raw[];

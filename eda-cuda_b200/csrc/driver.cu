@@ -123,6 +123,7 @@ void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) 
 
 Run::~Run() {
   if (dev_rows) cudaFree(dev_rows);
+  if (dev_orient) cudaFree(dev_orient);
 }
 
 namespace {
@@ -142,6 +143,27 @@ __global__ void collect_kernel(int64_t B, int32_t P, int32_t cap, int64_t count,
     else if (k <= n_imfs[b]) v = src[(b * cap + k) * count + i];
     else v = T(0);
     dst[idx] = v;
+  }
+}
+
+// dir (B, K, D, count) and coh (B, K, count) from the orientation rows (B, rows, D + 1, count): rows
+// k < n_imfs[b] of elements without an error, zero elsewhere.
+template <class T>
+__global__ void orient_collect_kernel(int64_t B, int32_t D, int64_t count, int32_t K, int32_t rows,
+                                      const int32_t* n_imfs, const int32_t* error, const T* __restrict__ src,
+                                      T* __restrict__ dir, T* __restrict__ coh) {
+  const int64_t total = B * K * (D + 1) * count;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx % count;
+    const int64_t q = idx / count;
+    const int32_t a = static_cast<int32_t>(q % (D + 1));
+    const int64_t bk = q / (D + 1);
+    const int64_t k = bk % K;
+    const int64_t b = bk / K;
+    const T v = error[b] == 0 && k < n_imfs[b] ? src[((b * rows + k) * (D + 1) + a) * count + i] : T(0);
+    if (a < D) dir[(bk * D + a) * count + i] = v;
+    else coh[bk * count + i] = v;
   }
 }
 
@@ -168,6 +190,74 @@ void Run::collect(void* dst, bool dst_on_device, cudaStream_t s) {
   } else {
     collect_kernel<double><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, meta, meta + batch,
                                                      static_cast<const double*>(dev_rows), static_cast<double*>(out));
+  }
+  EDAB_LAUNCH("collect_kernel");
+  if (!dst_on_device) {
+    copy_to_pageable(dst, out, elems * es, s);
+    EDAB_CUDA(cudaFreeAsync(out, s));
+  }
+  EDAB_CUDA(cudaFreeAsync(meta, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+}
+
+void Run::collect_orientation(void* dir, void* coh, bool dst_on_device, cudaStream_t s) {
+  if (!dev_orient) throw std::invalid_argument("eda: the call kept no orientation (return_orientation)");
+  const int32_t D = geom.dim;
+  if (batch == 0 || K == 0) return;
+  const size_t es = dtype == 0 ? 4 : 8;
+  const size_t nd = static_cast<size_t>(batch) * K * D * static_cast<size_t>(count);
+  const size_t nc = static_cast<size_t>(batch) * K * static_cast<size_t>(count);
+  int32_t* meta = nullptr;
+  EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&meta), sizeof(int32_t) * 2 * batch, s));
+  EDAB_CUDA(cudaMemcpyAsync(meta, n_imfs.data(), sizeof(int32_t) * batch, cudaMemcpyHostToDevice, s));
+  EDAB_CUDA(cudaMemcpyAsync(meta + batch, error.data(), sizeof(int32_t) * batch, cudaMemcpyHostToDevice, s));
+  void* d = dir;
+  void* c = coh;
+  if (!dst_on_device) {
+    EDAB_CUDA(cudaMallocAsync(&d, nd * es, s));
+    EDAB_CUDA(cudaMallocAsync(&c, nc * es, s));
+  }
+  const unsigned grid = std::min<unsigned>(blocks_for(static_cast<int64_t>(nd + nc) / 4 + 1), 1u << 20);
+  if (dtype == 0) {
+    orient_collect_kernel<float><<<grid, kThreads, 0, s>>>(batch, D, count, K, rows_cap - 1, meta, meta + batch,
+                                                           static_cast<const float*>(dev_orient),
+                                                           static_cast<float*>(d), static_cast<float*>(c));
+  } else {
+    orient_collect_kernel<double><<<grid, kThreads, 0, s>>>(batch, D, count, K, rows_cap - 1, meta, meta + batch,
+                                                            static_cast<const double*>(dev_orient),
+                                                            static_cast<double*>(d), static_cast<double*>(c));
+  }
+  EDAB_LAUNCH("orient_collect_kernel");
+  if (!dst_on_device) {
+    copy_to_pageable(dir, d, nd * es, s);
+    copy_to_pageable(coh, c, nc * es, s);
+    EDAB_CUDA(cudaFreeAsync(d, s));
+    EDAB_CUDA(cudaFreeAsync(c, s));
+  }
+  EDAB_CUDA(cudaFreeAsync(meta, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+}
+
+void Run::collect_one(int64_t j, void* dst, bool dst_on_device, cudaStream_t s) {
+  if (j < 0 || j >= batch) throw std::invalid_argument("eda: element index out of range");
+  const size_t es = dtype == 0 ? 4 : 8;
+  const int32_t P = rows_of(j);
+  const size_t elems = static_cast<size_t>(P) * static_cast<size_t>(count);
+  int32_t* meta = nullptr;
+  EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&meta), sizeof(int32_t) * 2, s));
+  EDAB_CUDA(cudaMemcpyAsync(meta, n_imfs.data() + j, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  EDAB_CUDA(cudaMemcpyAsync(meta + 1, error.data() + j, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  void* out = dst;
+  if (!dst_on_device) EDAB_CUDA(cudaMallocAsync(&out, elems * es, s));
+  const unsigned grid = std::min<unsigned>(blocks_for(static_cast<int64_t>(elems) / 4 + 1), 1u << 20);
+  const size_t off = static_cast<size_t>(j) * static_cast<size_t>(rows_cap) * static_cast<size_t>(count);
+  if (dtype == 0) {
+    collect_kernel<float><<<grid, kThreads, 0, s>>>(1, P, rows_cap, count, meta, meta + 1,
+                                                    static_cast<const float*>(dev_rows) + off, static_cast<float*>(out));
+  } else {
+    collect_kernel<double><<<grid, kThreads, 0, s>>>(1, P, rows_cap, count, meta, meta + 1,
+                                                     static_cast<const double*>(dev_rows) + off,
+                                                     static_cast<double*>(out));
   }
   EDAB_LAUNCH("collect_kernel");
   if (!dst_on_device) {
@@ -240,6 +330,16 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
     }
     EDAB_CUDA(e);
   }
+  if (p.orientation && dim >= 2) {
+    const size_t ob = static_cast<size_t>(batch) * (cap - 1) * (dim + 1) * static_cast<size_t>(g.count) * es;
+    const cudaError_t e = cudaMalloc(&run->dev_orient, ob);
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      throw OutOfMemory("eda: the orientation rows (" + std::to_string(ob >> 20) + " MiB) do not fit the device memory");
+    }
+    EDAB_CUDA(e);
+    EDAB_CUDA(cudaMemsetAsync(run->dev_orient, 0, ob, s));
+  }
   // the history: scale, sifts (int32), spacing, energy (double), [B, cap - 1] each
   int32_t* hist_i = nullptr;
   double* hist_d = nullptr;
@@ -252,7 +352,8 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
   if (p.max_chunk > 0) Bc = std::min(Bc, p.max_chunk);
   size_t free_b = 0, total_b = 0;
   EDAB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  const size_t margin = std::max<size_t>(size_t{256} << 20, free_b / 20);
+  if (p.mem_budget > 0) free_b = std::min(free_b, static_cast<size_t>(p.mem_budget));
+  const size_t margin = std::max<size_t>(p.mem_budget > 0 ? size_t{64} << 20 : size_t{256} << 20, free_b / 20);
   const auto need = [&](int64_t nb) {
     const Geom gc = make_geom(dim, nb, n);
     const size_t stage = static_cast<size_t>(nb) * static_cast<size_t>(g.count) * es;
@@ -291,12 +392,17 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     const size_t ho = static_cast<size_t>(b0) * static_cast<size_t>(cap - 1);
     unsigned char* rows0 = static_cast<unsigned char*>(run->dev_rows) + static_cast<size_t>(b0) * cap * g.count * es;
+    unsigned char* orient0 =
+        run->dev_orient ? static_cast<unsigned char*>(run->dev_orient) +
+                              static_cast<size_t>(b0) * (cap - 1) * (dim + 1) * static_cast<size_t>(g.count) * es
+                        : nullptr;
     if (f32) {
       run_chunk<float>(gc, c, s, ws, static_cast<const float*>(staged), reinterpret_cast<float*>(rows0), hist_i + ho,
-                       hist_i + he + ho, hist_d + ho, hist_d + he + ho, part);
+                       hist_i + he + ho, hist_d + ho, hist_d + he + ho, part, reinterpret_cast<float*>(orient0));
     } else {
       run_chunk<double>(gc, c, s, ws, static_cast<const double*>(staged), reinterpret_cast<double*>(rows0),
-                        hist_i + ho, hist_i + he + ho, hist_d + ho, hist_d + he + ho, part);
+                        hist_i + ho, hist_i + he + ho, hist_d + ho, hist_d + he + ho, part,
+                        reinterpret_cast<double*>(orient0));
     }
     for (int64_t b = 0; b < nb; ++b) elems[static_cast<size_t>(b0 + b)] = part[static_cast<size_t>(b)];
   }

@@ -65,6 +65,8 @@ struct Params {
   int32_t sifts = 3;
   bool check_finite = true;
   int64_t max_chunk = 0;
+  int64_t mem_budget = 0;  // > 0: the device bytes this call may hold (else the free memory)
+  bool orientation = false;  // keep n and c of every mode (D >= 2): return_orientation
 };
 
 // One call's results: the rows (B, cap, count) on the device and the per-element information.
@@ -77,10 +79,31 @@ struct Run {
   std::vector<int32_t> n_imfs, error, hist_scale, hist_sifts;
   std::vector<double> hist_spacing, hist_energy;
   void* dev_rows = nullptr;  // cudaMalloc'd
+  void* dev_orient = nullptr;  // (B, cap - 1, D + 1, count) with Params::orientation, cudaMalloc'd
   ~Run();
   // (B, P, count) into dst: NaN rows for failed elements, zeros above an element's residue.
   void collect(void* dst, bool dst_on_device, cudaStream_t s);
+  // Element j alone: (P_j, count) with P_j = n_imfs + 1 (1 for a failed element: a NaN row).
+  void collect_one(int64_t j, void* dst, bool dst_on_device, cudaStream_t s);
+  // return_orientation: dir (B, K, D, count) and coh (B, K, count), zero beyond n_imfs and for failed
+  // elements (cpp/src/method/orientation.cu:524-549, eda_orientation_collect).
+  void collect_orientation(void* dir, void* coh, bool dst_on_device, cudaStream_t s);
+  int32_t rows_of(int64_t j) const { return error[static_cast<size_t>(j)] ? 1 : n_imfs[static_cast<size_t>(j)] + 1; }
 };
+
+// A ragged batch: elements of different shapes, decomposed in groups of equal shape (an element's
+// results do not depend on the batch around it) by concurrent workers, each with its own stream
+// and workspace.
+struct RaggedRun {
+  int dtype = 0, dim = 1, device = 0;
+  std::vector<std::unique_ptr<Run>> groups;
+  std::vector<int32_t> group;   // per element: its group
+  std::vector<int64_t> index;   // per element: its index in the group
+};
+// xs[i]: element i, C-contiguous with extents n[i * dim .. i * dim + dim - 1]; on_device: every
+// element on the current device, ready once `s` reaches the call. workers: concurrent groups (>= 1).
+std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_device, int dtype, int dim, int64_t count,
+                                            const int64_t* n, const Params& p, int workers, cudaStream_t s);
 
 // Decomposes x (B, n_0..n_{D-1}), C-contiguous, float32 (dtype 0) or float64 (1), on the host or
 // the current device, on stream s. Throws std::invalid_argument, OutOfMemory or CudaError.
@@ -88,10 +111,17 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
                                const Params& p, cudaStream_t s);
 void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params& p);
 
+// eda.monogenic of the batch x (host or current device, C-contiguous (batch, n..)): out (host or
+// device) receives the planes amplitude, phase, frequency [batch][count], then in 2-D / 3-D
+// direction [batch][D][count] and coherence [batch][count]; nonfinite[b] (host) = 1 where element b
+// holds inf or NaN. Complete on return.
+void monogenic(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n, int64_t max_chunk,
+               void* out, bool out_on_device, int32_t* nonfinite, cudaStream_t s);
+
 template <class T>
 size_t engine_bytes(const Geom& g);
 template <class T>
 void run_chunk(const Geom& g, const Ctl& c, cudaStream_t s, Workspace& ws, const T* x, T* rows, int32_t* hs,
-               int32_t* hf, double* hp, double* he, std::vector<Elem>& out);
+               int32_t* hf, double* hp, double* he, std::vector<Elem>& out, T* orient = nullptr);
 
 }  // namespace edab

@@ -262,6 +262,11 @@ __host__ __device__ inline int32_t reflect_index(int32_t e, int32_t n) {
   return e < 0 ? -e - 1 : (e >= n ? 2 * n - 1 - e : e);
 }
 __host__ __device__ inline int64_t reflect_any(int64_t i, int64_t n) {
+  // within one reflection of the line (every segment point but those of windows longer than the
+  // line) without the 64-bit modulo, which the GPU emulates in a long instruction sequence
+  if (i >= 0 && i < n) return i;
+  if (i < 0 && i >= -n) return -i - 1;
+  if (i >= n && i < 2 * n) return 2 * n - 1 - i;
   const int64_t m = floor_mod(i, 2 * n);
   return m < n ? m : 2 * n - 1 - m;
 }

@@ -506,6 +506,8 @@ template <class T>
 class Engine {
  public:
   Engine(const Geom& g, const Ctl& c, cudaStream_t s, Workspace& ws) : g_(g), c_(c), s_(s) { bind(ws); }
+  // return_orientation: rows (B, rows_cap - 1, D + 1, count) receiving n and c of every mode
+  T* orient_out_ = nullptr;
 
   // x: the chunk's input, dense (B, count) on the device. Rows into rows_out (B, cap, count).
   void run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_sifts, double* hist_spacing,
@@ -560,6 +562,7 @@ class Engine {
   void g2();
   void g2_test(const uint8_t* ff, uint8_t* P);
   void orientation_and_build();
+  void store_orientation();
   bool ladder_and_weights(int32_t* n_rungs_max);
   void op(int which, const T* in, T* out0, T* out1, int32_t n_rungs_max);
   void envelope_mean(const T* h, T* m, T* u, T* l, int32_t nrm);
@@ -1005,6 +1008,7 @@ void Engine<T>::orientation_and_build() {
     for_elements(s_, B_, [=] __device__(int64_t b) {
       if (el[b].status == kActive && el[b].nonfinite) fail2(el[b], win_s, mask_s, B, b);
     });
+    if (orient_out_) store_orientation();
   }
   const dim3 grid = voxel_grid(g_);
   switch (g_.dim) {
@@ -1013,6 +1017,35 @@ void Engine<T>::orientation_and_build() {
     default: build_kernel<T, 3><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, n_[0], n_[1], n_[2], o_[0], o_[1], o_[2], el_, on); break;
   }
   EDAB_LAUNCH("build_kernel");
+}
+
+// return_orientation: n with the canonical sign (the first component of magnitude above the dtype's
+// default tie tolerance positive) and c at the row of this mode's IMF, unpadded, for every element
+// still active (cpp/src/method/orientation.cu:412-418, 495-522; driver.cpp:553-559).
+template <class T>
+void Engine<T>::store_orientation() {
+  const Elem* el = el_;
+  const Geom g = g_;
+  const int32_t D = g_.dim;
+  const int32_t rows = c_.rows_cap - 1;
+  const T zero = static_cast<T>(std::is_same_v<T, float> ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
+  const T* n0 = n_[0];
+  const T* n1 = n_[1];
+  const T* n2 = n_[2];
+  const T* coh = coh_;
+  T* out = orient_out_;
+  const int32_t nl = g_.n_last;
+  for_voxels(s_, g_, [=] __device__(int64_t b) { return el[b].status == kActive; },
+             [=] __device__(int64_t b, int64_t v, int64_t i) {
+               T nt[3] = {n0[i], n1[i], D >= 3 ? n2[i] : T(0)};
+               int sg = 0;
+               for (int a = 0; a < D; ++a) sg = sg == 0 && fabs(nt[a]) > zero ? (nt[a] > T(0) ? 1 : -1) : sg;
+               const int64_t q = pitch_row(g, v);
+               const int64_t t = v - q * g.pitch;
+               T* o = out + ((b * rows + el[b].n_imfs) * (D + 1)) * g.count + q * nl + t;
+               for (int a = 0; a < D; ++a) o[a * g.count] = sg < 0 ? -nt[a] : nt[a];
+               o[D * g.count] = coh[i];
+             });
 }
 
 // S4: the ladders (host), then the rung logs, the weights and the rung windows.
@@ -1593,16 +1626,17 @@ size_t engine_bytes(const Geom& g) {
 
 template <class T>
 void run_chunk(const Geom& g, const Ctl& c, cudaStream_t s, Workspace& ws, const T* x, T* rows, int32_t* hs,
-               int32_t* hf, double* hp, double* he, std::vector<Elem>& out) {
+               int32_t* hf, double* hp, double* he, std::vector<Elem>& out, T* orient) {
   Engine<T> e(g, c, s, ws);
+  e.orient_out_ = g.dim >= 2 ? orient : nullptr;
   e.run(x, rows, hs, hf, hp, he, out);
 }
 
 template size_t engine_bytes<float>(const Geom&);
 template size_t engine_bytes<double>(const Geom&);
 template void run_chunk<float>(const Geom&, const Ctl&, cudaStream_t, Workspace&, const float*, float*, int32_t*,
-                               int32_t*, double*, double*, std::vector<Elem>&);
+                               int32_t*, double*, double*, std::vector<Elem>&, float*);
 template void run_chunk<double>(const Geom&, const Ctl&, cudaStream_t, Workspace&, const double*, double*,
-                                int32_t*, int32_t*, double*, double*, std::vector<Elem>&);
+                                int32_t*, int32_t*, double*, double*, std::vector<Elem>&, double*);
 
 }  // namespace edab

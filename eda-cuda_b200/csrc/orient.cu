@@ -115,6 +115,17 @@ RotPass make_pass(const Geom& g, const Layout& L) {
   RotPass p{};
   p.K = g.n[L.ax[D - 1]];
   p.pitch_in = pad32(p.K);
+  if (D == 1) {
+    // one axis: every element is one row, stored in place (no rotation)
+    p.rows = 1;
+    p.f_in = p.pitch_in;
+    p.n_lo = 1;
+    p.pitch_out = 1;
+    p.s_j = 1;
+    p.f_out = p.pitch_in;
+    p.M = g.batch;
+    return p;
+  }
   p.rows = 1;
   for (int i = 0; i < D - 1; ++i) p.rows *= g.n[L.ax[i]];
   p.f_in = p.rows * p.pitch_in;
@@ -551,6 +562,192 @@ void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T*
   else tensor_eigen<T, 3><<<grid, 256, 0, s>>>(g, run, R1, R2, n[0], n[1], n[2], coh, el);
   EDAB_LAUNCH("tensor_eigen");
 }
+
+// ---------------------------------------------------------------------------------------------
+// eda.monogenic (cpp/src/method/orientation.cu:420-493, 791-831 of eda-cuda): the Riesz components
+// of the whole spectrum (no band) of the prescaled field f, the orientation's eigen step (D >= 2),
+// then per sample, in double and in the reference's order: n canonical (1 in 1-D), q = sum n_a R1_a,
+// A^2 = f^2 + sum R1_a^2, D_n f = sum n_b D_b f, D_n q = sum_{a <= b} m_ab D_b R_a (m_aa = n_a^2,
+// m_ab = 2 n_a n_b); where A^2 > tiny: phase = atan2(q, f) (an angle that rounds to -pi is pi),
+// frequency = (f D_n q - q D_n f) / A^2; amplitude = sqrt(A^2) 2^exp, rounded once.
+namespace {
+
+// The Riesz multiplier of component (kind, a, b) at the spectrum index k (riesz_mult, orientation.cu:
+// 116-127): 0 R1_a, 1 R2_aa, 2 R2_ab, 3 D_a f, 4 D_b R_a; 0 at the DC.
+template <int D>
+__device__ __forceinline__ double riesz_mult(const Geom& g, int kind, int a, int b, const int32_t* k) {
+  double u[kMaxDim];
+  const double rad = dct_freq<D>(g, k, u);
+  if (!(rad > 0.0)) return 0.0;
+  const double inv = __ddiv_rn(1.0, rad);
+  const double ua = __dmul_rn(u[a], inv);
+  if (kind == 0) return ua;
+  if (kind == 1) return __dmul_rn(-ua, ua);
+  if (kind == 3) return -u[a];
+  if (kind == 4) return a == b ? __dmul_rn(u[a], ua) : -__dmul_rn(u[a], __dmul_rn(u[b], inv));
+  return __dmul_rn(ua, __dmul_rn(u[b], inv));
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(256) riesz_spectrum(Geom g, int kind, int a, int b, const T* __restrict__ X,
+                                                      T* __restrict__ Y) {
+  for (int64_t e = blockIdx.y; e < g.batch; e += gridDim.y) {
+    for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
+         v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      int32_t k[kMaxDim];
+      if (!voxel_coords_d<D>(g, v, k)) continue;
+      const int64_t i = e * g.field + v;
+      Y[i] = static_cast<T>(__dmul_rn(riesz_mult<D>(g, kind, a, b, k), static_cast<double>(X[i])));
+    }
+  }
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(256) monogenic_kernel(Geom g, const T* __restrict__ f, const T* r1,
+                                                        const T* df, const T* dr, const T* n, const T* c,
+                                                        const int32_t* __restrict__ exp, double tiny, T zero,
+                                                        T* __restrict__ out, int64_t out_batch, int64_t b0) {
+  constexpr int NP = D * (D + 1) / 2;
+  const int64_t F = g.batch * g.field;
+  const int64_t plane = out_batch * g.count;
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
+    for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
+         v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const int64_t row = pitch_row(g, v), col = v - row * g.pitch;
+      if (col >= g.n_last) continue;
+      const int64_t i = b * g.field + v;
+      T nt[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) nt[a] = D == 1 ? T(1) : n[a * F + i];
+      if constexpr (D >= 2) {
+        int sg = 0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) sg = sg == 0 && fabs(nt[a]) > zero ? (nt[a] > T(0) ? 1 : -1) : sg;
+#pragma unroll
+        for (int a = 0; a < D; ++a) nt[a] = sg < 0 ? -nt[a] : nt[a];
+      }
+      const double fv = static_cast<double>(f[i]);
+      double q = 0.0, a2 = __dmul_rn(fv, fv), dnf = 0.0, dnq = 0.0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const double na = static_cast<double>(nt[a]);
+        const double r = static_cast<double>(r1[a * F + i]);
+        q = __dadd_rn(q, __dmul_rn(na, r));
+        a2 = __dadd_rn(a2, __dmul_rn(r, r));
+        dnf = __dadd_rn(dnf, __dmul_rn(na, static_cast<double>(df[a * F + i])));
+      }
+      int p = 0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+#pragma unroll
+        for (int cc = a; cc < D; ++cc, ++p) {
+          const double na = static_cast<double>(nt[a]), nc = static_cast<double>(nt[cc]);
+          const double m = a == cc ? __dmul_rn(na, na) : __dmul_rn(2.0, __dmul_rn(na, nc));
+          dnq = __dadd_rn(dnq, __dmul_rn(m, static_cast<double>(dr[p * F + i])));
+        }
+      }
+      (void)NP;
+      double phase = 0.0, freq = 0.0;
+      if (a2 > tiny) {
+        phase = atan2(q, fv);
+        freq = __ddiv_rn(__dsub_rn(__dmul_rn(fv, dnq), __dmul_rn(q, dnf)), a2);
+      }
+      const int64_t at = (b0 + b) * g.count + row * g.n_last + col;
+      out[at] = static_cast<T>(ldexp(__dsqrt_rn(a2), exp[b]));
+      const T pt = static_cast<T>(phase);
+      out[plane + at] = pt == -static_cast<T>(pi) ? static_cast<T>(pi) : pt;
+      out[2 * plane + at] = static_cast<T>(freq);
+      if constexpr (D >= 2) {
+        const int64_t e = (b0 + b) * D * g.count + row * g.n_last + col;
+#pragma unroll
+        for (int a = 0; a < D; ++a) out[3 * plane + e + a * g.count] = nt[a];
+        out[(3 + D) * plane + at] = c[i];
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int64_t monogenic_work_samples(const Geom& g) {
+  const int D = g.dim;
+  const int64_t P = D * (D + 1) / 2;
+  return 3 * g.batch * orient_layout_samples(g) + (2 * D + (D >= 2 ? P : 0) + P + (D >= 2 ? D + 1 : 0)) * g.batch * g.field;
+}
+
+template <class T>
+void monogenic_fields(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* f, const int32_t* run,
+                      const int32_t* exp, Elem* el, T* work, T* out, int64_t out_batch, int64_t b0, int32_t* err) {
+  const int D = g.dim;
+  const int64_t F = g.batch * g.field;
+  const int64_t Fw = g.batch * orient_layout_samples(g);
+  const int P = D * (D + 1) / 2;
+  T* X = work;
+  T* Y = X + Fw;
+  T* Z = Y + Fw;
+  T* R1 = Z + Fw;      // D fields
+  T* DF = R1 + D * F;  // D fields
+  T* R2 = DF + D * F;  // P fields (D >= 2)
+  T* DR = R2 + (D >= 2 ? P : 0) * F;  // P fields
+  T* N = DR + P * F;   // D fields (D >= 2)
+  T* C = N + D * F;    // 1 field (D >= 2)
+  // the mean (double), then f - mean rounded to T, then the forward DCT-II of every axis
+  const int64_t nchunks = (g.field + kMeanChunk - 1) / kMeanChunk;
+  double* mean = reinterpret_cast<double*>(Z);
+  double* part = mean + g.batch;
+  mean_partial<T><<<dim3(static_cast<unsigned>(nchunks), static_cast<unsigned>(g.batch)), 256, 0, s>>>(g, f, run, part,
+                                                                                                       nchunks);
+  EDAB_LAUNCH("mean_partial");
+  mean_final<<<blocks_for(g.batch), 256, 0, s>>>(g.batch, g.count, run, part, nchunks, mean);
+  EDAB_LAUNCH("mean_final");
+  for_voxels(s, g, [=] __device__(int64_t b) { return run[b] != 0; },
+             [=] __device__(int64_t b, int64_t, int64_t i) {
+               Y[i] = static_cast<T>(__dsub_rn(static_cast<double>(f[i]), mean[b]));
+             });
+  int kinds[kMaxDim] = {0, 0, 0};
+  transform_axes<T>(s, g, plan, Y, X, Z, Y, kinds, run, err);
+  const dim3 grid = voxel_grid(g);
+  auto component = [&](int kind, int a, int b, T* dst) {
+    switch (D) {
+      case 1: riesz_spectrum<T, 1><<<grid, 256, 0, s>>>(g, kind, a, b, X, Y); break;
+      case 2: riesz_spectrum<T, 2><<<grid, 256, 0, s>>>(g, kind, a, b, X, Y); break;
+      default: riesz_spectrum<T, 3><<<grid, 256, 0, s>>>(g, kind, a, b, X, Y); break;
+    }
+    EDAB_LAUNCH("riesz_spectrum");
+    const int odd = (kind == 0 || kind == 3) ? (1 << a) : (a == b ? 0 : ((1 << a) | (1 << b)));
+    int kk[kMaxDim] = {1, 1, 1};
+    for (int ax = 0; ax < D; ++ax) kk[ax] = ((odd >> ax) & 1) ? 2 : 1;
+    transform_axes<T>(s, g, plan, Y, dst, Z, Y, kk, run, err);
+  };
+  for (int a = 0; a < D; ++a) {
+    component(0, a, a, R1 + a * F);
+    component(3, a, a, DF + a * F);
+  }
+  int p = 0;
+  for (int a = 0; a < D; ++a) {
+    for (int b = a; b < D; ++b, ++p) {
+      if (D >= 2) component(a == b ? 1 : 2, a, b, R2 + p * F);
+      component(4, a, b, DR + p * F);
+    }
+  }
+  if (D == 2) tensor_eigen<T, 2><<<grid, 256, 0, s>>>(g, run, R1, R2, N, N + F, nullptr, C, el);
+  else if (D == 3) tensor_eigen<T, 3><<<grid, 256, 0, s>>>(g, run, R1, R2, N, N + F, N + 2 * F, C, el);
+  if (D >= 2) EDAB_LAUNCH("tensor_eigen");
+  const double tiny = std::is_same_v<T, float> ? 1.17549435082228750797e-38 : 1e-300;
+  const T zero = static_cast<T>(std::is_same_v<T, float> ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
+  switch (D) {
+    case 1: monogenic_kernel<T, 1><<<grid, 256, 0, s>>>(g, f, R1, DF, DR, N, C, exp, tiny, zero, out, out_batch, b0); break;
+    case 2: monogenic_kernel<T, 2><<<grid, 256, 0, s>>>(g, f, R1, DF, DR, N, C, exp, tiny, zero, out, out_batch, b0); break;
+    default: monogenic_kernel<T, 3><<<grid, 256, 0, s>>>(g, f, R1, DF, DR, N, C, exp, tiny, zero, out, out_batch, b0); break;
+  }
+  EDAB_LAUNCH("monogenic_kernel");
+}
+
+template void monogenic_fields<float>(cudaStream_t, const Geom&, const OrientPlan&, const float*, const int32_t*,
+                                      const int32_t*, Elem*, float*, float*, int64_t, int64_t, int32_t*);
+template void monogenic_fields<double>(cudaStream_t, const Geom&, const OrientPlan&, const double*, const int32_t*,
+                                       const int32_t*, Elem*, double*, double*, int64_t, int64_t, int32_t*);
 
 template void orientation<float>(cudaStream_t, const Geom&, const OrientPlan&, const float*, Elem*, const int32_t*,
                                  float* const*, float*, float*, double, int32_t*);

@@ -68,4 +68,13 @@ template <class T>
 void orientation(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* r, Elem* el, const int32_t* run,
                  T* const* n, T* coh, T* work, double two_sigma2, int32_t* err);
 
+// eda.monogenic of the prescaled fields f (element layout; f = x 2^-exp[b]) of the elements with
+// run[b]: the planes of out (out_batch elements; this chunk at b0): amplitude, phase, frequency
+// [out_batch][count], then in 2-D / 3-D direction [out_batch][D][count] and coherence. work holds
+// monogenic_work_samples(g) samples.
+int64_t monogenic_work_samples(const Geom& g);
+template <class T>
+void monogenic_fields(cudaStream_t s, const Geom& g, const OrientPlan& plan, const T* f, const int32_t* run,
+                      const int32_t* exp, Elem* el, T* work, T* out, int64_t out_batch, int64_t b0, int32_t* err);
+
 }  // namespace edab

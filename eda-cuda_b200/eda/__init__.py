@@ -10,7 +10,7 @@ import operator
 from typing import Any
 
 from . import _native
-from ._api import DecompositionInfo, decompose
+from ._api import DecompositionInfo, Monogenic, Orientation, decompose, decompose_ragged, monogenic
 from ._device import DeviceArray
 from ._errors import CudaError, DecompositionError
 
@@ -21,11 +21,15 @@ __all__ = [
     "DecompositionError",
     "DecompositionInfo",
     "DeviceArray",
+    "Monogenic",
+    "Orientation",
     "__version__",
     "build_info",
     "decompose",
+    "decompose_ragged",
     "device_count",
     "device_info",
+    "monogenic",
 ]
 
 

@@ -31,6 +31,7 @@ class _Params(ctypes.Structure):
         ("sifts", ctypes.c_int32),
         ("check_finite", ctypes.c_int32),
         ("max_chunk", ctypes.c_int64),
+        ("orientation", ctypes.c_int32),
     ]
 
 
@@ -46,12 +47,21 @@ class Core:
                                     ctypes.POINTER(i64), ctypes.POINTER(i64)]
         L.eda_run_info.argtypes = [vp] + [vp] * 6
         L.eda_run_collect.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.eda_run_collect_orientation.argtypes = [vp, vp, vp, ctypes.c_int, vp]
         L.eda_run_free.argtypes = [vp]
         L.eda_run_free.restype = None
         L.eda_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         L.eda_last_error.restype = ctypes.c_size_t
         L.eda_build_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         L.eda_device_info.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+        L.eda_decompose_ragged.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, i64,
+                                           ctypes.POINTER(i64), ctypes.POINTER(_Params), i32, vp, ctypes.POINTER(vp)]
+        L.eda_ragged_element.argtypes = [vp, i64] + [vp] * 7
+        L.eda_ragged_collect.argtypes = [vp, i64, vp, ctypes.c_int, vp]
+        L.eda_monogenic.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, i64, ctypes.POINTER(i64), i64, vp,
+                                    ctypes.c_int, ctypes.POINTER(i32), vp]
+        L.eda_ragged_free.argtypes = [vp]
+        L.eda_ragged_free.restype = None
         self._lib = L
         self.path = str(path)
 
@@ -91,9 +101,10 @@ class Core:
 
     # -- the decomposition ---------------------------------------------------------------------
     def _run(self, ptr: int, on_device: bool, dtype: np.dtype, shape: tuple[int, ...], max_imf: int,
-             tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int, stream: int):
+             tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int, stream: int,
+             orientation: bool = False):
         p = _Params(int(max_imf), -1.0 if tie_tolerance is None else float(tie_tolerance), int(sifts),
-                    int(bool(check_finite)), int(max_chunk))
+                    int(bool(check_finite)), int(max_chunk), int(bool(orientation)))
         n = (ctypes.c_int64 * 3)(*[int(v) for v in shape[1:]], *([1] * (4 - len(shape))))
         run = ctypes.c_void_p()
         code = 0 if dtype == np.float32 else 1
@@ -126,8 +137,6 @@ class Core:
                        check_finite: bool, orientation: bool, max_chunk: int) -> tuple:
         """Decomposes the C-contiguous host array x (B, *spatial) of float32 or float64:
         (rows (B, P, *spatial), info)."""
-        if orientation:
-            raise NotImplementedError("eda: return_orientation is not available in the B200 engine")
         if not (isinstance(x, np.ndarray) and x.flags.c_contiguous and x.dtype in (np.float32, np.float64)):
             raise TypeError("eda: decompose_host: expected a C-contiguous float32 or float64 array")
         if x.ndim < 2 or x.ndim > 4:
@@ -136,11 +145,19 @@ class Core:
             self._validate_empty(x, max_imf, tie_tolerance, sifts, check_finite, max_chunk)
             return np.zeros((0, 1) + x.shape[1:], x.dtype), self._empty_info(0)
         run = self._run(x.ctypes.data, False, x.dtype, x.shape, max_imf, tie_tolerance, sifts, check_finite,
-                        max_chunk, 0)
+                        max_chunk, 0, orientation)
         try:
             info, P, B, count = self._info(run)
             rows = np.empty((B, P) + x.shape[1:], x.dtype)
             self._check(self._lib.eda_run_collect(run, ctypes.c_void_p(rows.ctypes.data), 0, None))
+            if orientation:
+                K, D = info["windows"].shape[1], x.ndim - 1
+                info["direction"] = np.zeros((B, K, D) + x.shape[1:], x.dtype)
+                info["coherence"] = np.zeros((B, K) + x.shape[1:], x.dtype)
+                if K:
+                    self._check(self._lib.eda_run_collect_orientation(
+                        run, ctypes.c_void_p(info["direction"].ctypes.data),
+                        ctypes.c_void_p(info["coherence"].ctypes.data), 0, None))
         finally:
             self._lib.eda_run_free(run)
         return rows, info
@@ -157,18 +174,85 @@ class Core:
 
     def decompose_device(self, ptr: int, device: int, dtype: str, shape: tuple[int, ...], max_imf: int,
                          tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int,
-                         stream: int, out_ptr_of) -> tuple:
+                         stream: int, out_ptr_of, orient_of=None) -> tuple:
         """Decomposes the C-contiguous device array at ptr (B, *spatial) in the compute dtype on its
-        device; ``out_ptr_of(P)`` allocates the (B, P, *spatial) output and returns its pointer."""
+        device; ``out_ptr_of(P)`` allocates the (B, P, *spatial) output and returns it with its
+        pointer; with ``orient_of`` (return_orientation), ``orient_of(K)`` allocates the direction
+        (B, K, D, *spatial) and coherence (B, K, *spatial) outputs and returns them with their
+        pointers, kept in info["direction"] / info["coherence"]."""
         run = self._run(ptr, True, np.dtype(dtype), shape, max_imf, tie_tolerance, sifts, check_finite,
-                        max_chunk, stream)
+                        max_chunk, stream, orient_of is not None)
         try:
             info, P, B, count = self._info(run)
             out, out_ptr = out_ptr_of(P)
             self._check(self._lib.eda_run_collect(run, ctypes.c_void_p(out_ptr), 1, ctypes.c_void_p(stream)))
+            if orient_of is not None:
+                K = info["windows"].shape[1]
+                (d, d_ptr), (c, c_ptr) = orient_of(K)
+                if K:
+                    self._check(self._lib.eda_run_collect_orientation(run, ctypes.c_void_p(d_ptr),
+                                                                      ctypes.c_void_p(c_ptr), 1,
+                                                                      ctypes.c_void_p(stream)))
+                info["direction"], info["coherence"] = d, c
         finally:
             self._lib.eda_run_free(run)
         return out, info
+
+
+    def decompose_ragged(self, ptrs: list[int], on_device: bool, dtype: str, shapes: list[tuple[int, ...]],
+                         max_imf: int, tie_tolerance: float | None, sifts: int, check_finite: bool, workers: int,
+                         stream: int, out_of) -> list[tuple[Any, dict]]:
+        """Decomposes len(ptrs) C-contiguous arrays of one dtype and one number of axes, each of its own
+        shape, on the host or on the current device (ready once ``stream`` reaches the call);
+        ``out_of(P, shape)`` allocates an element's (P, *shape) output and returns it with its
+        pointer. Returns (rows, info) per element; info holds ``n_imfs``, ``error`` and the
+        ``windows``, ``sifts``, ``spacing``, ``energy`` of its IMFs."""
+        count = len(ptrs)
+        dim = len(shapes[0]) if count else 1
+        p = _Params(int(max_imf), -1.0 if tie_tolerance is None else float(tie_tolerance), int(sifts),
+                    int(bool(check_finite)), 0)
+        xs = (ctypes.c_void_p * max(count, 1))(*[ctypes.c_void_p(int(v)) for v in ptrs])
+        flat = [int(v) for sh in shapes for v in sh]
+        n = (ctypes.c_int64 * max(len(flat), 1))(*flat)
+        run = ctypes.c_void_p()
+        code = 0 if np.dtype(dtype) == np.float32 else 1
+        self._check(self._lib.eda_decompose_ragged(xs, int(on_device), code, dim, count, n, ctypes.byref(p),
+                                                   int(workers), ctypes.c_void_p(stream), ctypes.byref(run)))
+        out = []
+        try:
+            for i in range(count):
+                P, k, err = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+                self._check(self._lib.eda_ragged_element(run, i, ctypes.byref(P), ctypes.byref(k), ctypes.byref(err),
+                                                         None, None, None, None))
+                K = 0 if err.value else k.value
+                info = {"n_imfs": int(k.value), "error": int(err.value), "windows": np.zeros(K, np.int32),
+                        "sifts": np.zeros(K, np.int32), "spacing": np.zeros(K, np.float64),
+                        "energy": np.zeros(K, np.float64)}
+                self._check(self._lib.eda_ragged_element(
+                    run, i, None, None, None, *(ctypes.c_void_p(info[f].ctypes.data) for f in
+                                                ("windows", "sifts", "spacing", "energy"))))
+                rows, ptr = out_of(P.value, tuple(shapes[i]))
+                self._check(self._lib.eda_ragged_collect(run, i, ctypes.c_void_p(ptr), int(on_device),
+                                                         ctypes.c_void_p(stream)))
+                out.append((rows, info))
+        finally:
+            self._lib.eda_ragged_free(run)
+        return out
+
+
+    def monogenic(self, ptr: int, on_device: bool, dtype: str, shape: tuple[int, ...], stream: int, out_ptr: int,
+                  max_chunk: int = 0) -> np.ndarray:
+        """The monogenic planes of the C-contiguous (B, *spatial) array at ptr into the buffer at
+        out_ptr (host memory, or device memory for device input); returns the non-finite flags [B]."""
+        B = int(shape[0])
+        n = (ctypes.c_int64 * 3)(*[int(v) for v in shape[1:]], *([1] * (4 - len(shape))))
+        bad = np.zeros(max(B, 1), np.int32)
+        code = 0 if np.dtype(dtype) == np.float32 else 1
+        self._check(self._lib.eda_monogenic(ctypes.c_void_p(ptr), int(on_device), code, len(shape) - 1, B, n,
+                                            int(max_chunk), ctypes.c_void_p(out_ptr), int(on_device),
+                                            bad.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                            ctypes.c_void_p(stream)))
+        return bad[:B]
 
 
 def core() -> Core:

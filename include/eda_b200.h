@@ -50,6 +50,9 @@ typedef struct eda_params {
   int32_t sifts;          /* sifts per mode, >= 1 (3 by default) */
   int32_t check_finite;   /* non-zero: an element holding inf or NaN fails with code 1 */
   int64_t max_chunk;      /* > 0: at most this many elements per chunk; 0: by free device memory */
+  int32_t orientation;    /* non-zero (D >= 2): keep every mode's direction and coherence for
+                             eda_run_collect_orientation (the binding's orientation flag,
+                             cpp/python/decompose.cpp:325-509) */
 } eda_params;
 
 /* One call's results: the rows on the device and the per-element information (the reference's
@@ -80,7 +83,47 @@ EDA_API int eda_run_info(const eda_run* run, int32_t* n_imfs, int32_t* error, in
  * then the residue, zeros above (cpp/src/field/field_ops.hpp:43-47, Run::collect). */
 EDA_API int eda_run_collect(eda_run* run, void* dst, int dst_on_device, void* stream);
 
+/* return_orientation (a call with params->orientation and 2 or 3 axes): dir (batch, K, D, count)
+ * receives every mode's unit direction n across the stripes (component a along axis a; the first
+ * component of magnitude above the dtype's default tie tolerance positive) and coh (batch, K,
+ * count) its coherence in [0, 1], both as computed at the start of the mode; rows beyond an
+ * element's n_imfs and all rows of a failed element are 0 (cpp/src/decompose.hpp:97-104,
+ * Run::collect_orientation). Host or device memory of the run's device, complete on return. */
+EDA_API int eda_run_collect_orientation(eda_run* run, void* dir, void* coh, int dst_on_device, void* stream);
+
 EDA_API void eda_run_free(eda_run* run);
+
+/* eda.monogenic (cpp/src/method/monogenic.cpp:145-155, run_monogenic; the binding's monogenic_host /
+ * monogenic_device): the monogenic signal of every field of x (C-contiguous (batch, n[0], ..,
+ * n[dim-1]), float32 or float64, host or current device). out (host, or device with out_on_device)
+ * receives the reference's native planes: amplitude, phase (-pi, pi], frequency (cycles per sample
+ * along the direction), each [batch][count], then in 2-D / 3-D the direction [batch][D][count]
+ * (first component above the dtype's default tie tolerance positive) and the coherence
+ * [batch][count]; nonfinite[batch] (host) receives 1 for a field holding inf or NaN. max_chunk > 0
+ * caps the elements per chunk. Complete on return. */
+EDA_API int eda_monogenic(const void* x, int x_on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                          int64_t max_chunk, void* out, int out_on_device, int32_t* nonfinite, void* stream);
+
+/* Ragged batches: count elements of different shapes (same dtype and dim) in one call. Element i is
+ * the C-contiguous array x[i] with extents n[i * dim .. i * dim + dim - 1], all on the host
+ * (x_on_device 0) or all on the calling thread's current device and ready once `stream` (a
+ * cudaStream_t; NULL: the legacy default stream) reaches the call. Equal shapes are decomposed
+ * together and up to `workers` groups run concurrently, each on its own stream and workspace; every
+ * element's rows and information are those a one-element eda_decompose call gives. The reference
+ * takes one shape per call (cpp/src/decompose.hpp:106): a ragged workload there is one call per
+ * shape. On EDA_OK *out receives the run, released by eda_ragged_free. */
+typedef struct eda_ragged_run eda_ragged_run;
+EDA_API int eda_decompose_ragged(const void* const* x, int x_on_device, int dtype, int dim, int64_t count,
+                                 const int64_t* n, const eda_params* params, int32_t workers, void* stream,
+                                 eda_ragged_run** out);
+/* Element i's rows P (n_imfs + 1, or 1 for a failed element), n_imfs, error, and its windows,
+ * sifts, spacing, energy (n_imfs entries each, none for a failed element; any pointer may be NULL). */
+EDA_API int eda_ragged_element(const eda_ragged_run* run, int64_t i, int32_t* rows, int32_t* n_imfs, int32_t* error,
+                               int32_t* windows, int32_t* sifts, double* spacing, double* energy);
+/* Element i's rows (P, *n_i) into dst (host, or device memory of the run's device), complete on
+ * return: a NaN row for a failed element, the IMFs then the residue otherwise. */
+EDA_API int eda_ragged_collect(eda_ragged_run* run, int64_t i, void* dst, int dst_on_device, void* stream);
+EDA_API void eda_ragged_free(eda_ragged_run* run);
 
 /* The calling thread's last error message (NUL-terminated, truncated to len). Returns its full
  * length. */

@@ -408,6 +408,94 @@ struct Result {
   std::vector<double> spacing, energy;
 };
 
+// The energy tensor T = R1 R1^T + R2 R2^T in T and its Jacobi eigen-decomposition in double
+// (cpp/src/method/element.cu:49-164): nf[a] the top eigenvector, coh = (mu1 - mu2) / (mu1 + mu2)
+// clipped to [0, 1]; *nonfinite set when a tensor entry is not finite.
+template <class T>
+void orientation_eigen(int D, int64_t N, const std::vector<T>* R1, const std::vector<T>* R2, std::vector<T>* nf,
+                       std::vector<T>& coh, bool* nonfinite) {
+  const auto pair = [D](int a, int b) {
+    if (a > b) std::swap(a, b);
+    return D == 2 ? (a == 0 ? b : 2) : (a == 0 ? b : (a == 1 ? 2 + b : 5));
+  };
+  for (int a = 0; a < D; ++a) nf[a].assign(static_cast<size_t>(N), T(0));
+  coh.assign(static_cast<size_t>(N), T(0));
+  for (int64_t i = 0; i < N; ++i) {
+    // the tensor in T: v = R1_a R1_c, then + h(a, k) h(k, c) for k = 0..D-1
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    bool finite = true;
+    for (int a = 0; a < D; ++a) {
+      for (int c = a; c < D; ++c) {
+        T v = R1[a][i] * R1[c][i];
+        for (int k = 0; k < D; ++k) v = v + static_cast<T>(R2[pair(a, k)][i] * R2[pair(k, c)][i]);
+        A[a][c] = A[c][a] = static_cast<double>(v);
+        finite = finite && std::isfinite(A[a][c]);
+      }
+    }
+    if (!finite) *nonfinite = true;
+    // Jacobi (element.cu:49-164): one rotation in 2-D; 6 cyclic sweeps after a power-of-two
+    // prescale in 3-D
+    const auto rotate = [&](int pp, int q, int rr, int dim) {
+      const double apq = A[pp][q];
+      if (apq == 0.0) return;
+      const double theta = (A[q][q] - A[pp][pp]) / (2.0 * apq);
+      const double at = std::fabs(theta);
+      const double t = std::copysign(1.0, theta) / (at + std::sqrt(theta * theta + 1.0));
+      const double cc = 1.0 / std::sqrt(t * t + 1.0);
+      const double s = t * cc;
+      const double tau = s / (1.0 + cc);
+      const double tapq = t * apq;
+      A[pp][pp] = A[pp][pp] - tapq;
+      A[q][q] = A[q][q] + tapq;
+      A[pp][q] = A[q][pp] = 0.0;
+      if (rr >= 0) {
+        const double gg = A[rr][pp], hh = A[rr][q];
+        const double np_ = gg - s * (hh + gg * tau);
+        const double nq_ = hh + s * (gg - hh * tau);
+        A[rr][pp] = A[pp][rr] = np_;
+        A[rr][q] = A[q][rr] = nq_;
+      }
+      for (int k = 0; k < dim; ++k) {
+        const double gg = V[k][pp], hh = V[k][q];
+        V[k][pp] = gg - s * (hh + gg * tau);
+        V[k][q] = hh + s * (gg - hh * tau);
+      }
+    };
+    if (D == 2) {
+      rotate(0, 1, -1, 2);
+    } else {
+      double am = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        for (int c = a; c < 3; ++c) am = std::fmax(am, std::fabs(A[a][c]));
+      }
+      if (am > 0.0 && am < INFINITY) {
+        const double sc = std::scalbn(1.0, -std::ilogb(am));
+        for (int a = 0; a < 3; ++a) {
+          for (int c = 0; c < 3; ++c) A[a][c] = A[a][c] * sc;
+        }
+      }
+      for (int sweep = 0; sweep < 6; ++sweep) {
+        rotate(0, 1, 2, 3);
+        rotate(0, 2, 1, 3);
+        rotate(1, 2, 0, 3);
+      }
+    }
+    double mu[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < D; ++a) mu[a] = A[a][a];
+    int top = 0;
+    for (int a = 1; a < D; ++a) top = mu[a] > mu[top] ? a : top;
+    double mu2 = -INFINITY;
+    for (int a = 0; a < D; ++a) mu2 = (a != top && mu[a] > mu2) ? mu[a] : mu2;
+    const double mu1 = mu[top];
+    const double ssum = mu1 + mu2;
+    double cv = ssum > 0.0 ? (mu1 - mu2) / ssum : 0.0;
+    cv = cv < 0.0 ? 0.0 : (cv > 1.0 ? 1.0 : cv);
+    coh[i] = static_cast<T>(cv);
+    for (int a = 0; a < D; ++a) nf[a][i] = static_cast<T>(V[a][top]);
+  }
+}
+
 template <class T>
 class Element {
  public:
@@ -417,6 +505,9 @@ class Element {
 
   // Runs the decomposition of x (count samples) into rows (cap x count): IMFs, then the residue.
   Result run(const T* x, T* rows);
+  // With return_orientation: rows (cap - 1, D + 1, count) receive n (canonical sign) and c of every
+  // mode at the row of its IMF (cpp/src/method/driver.cpp:553-559; orientation.cu:495-522).
+  void keep_orientation(T* orient) { orient_ = orient; }
 
  private:
   using F = std::vector<T>;
@@ -425,6 +516,7 @@ class Element {
   const double tau_;
   const bool check_finite_;
   const int32_t max_imf_, cap_;
+  T* orient_ = nullptr;
   // per-element record (cpp/src/method/method.hpp:94-132)
   int32_t k_ = 0, w_prev_ = 1, w_ = 0, W_ = 0, fine_ = 0, p_odd_ = 0, n_rungs_ = 0, n_sifts_ = 0;
   uint64_t ext_[kMaxDim] = {0, 0, 0};
@@ -863,86 +955,9 @@ void Element<T>::orientation(const F& r, F* nf, F& coh) {
   for (int a = 0; a < D; ++a) {
     for (int b = a; b < D; ++b, ++p) R2[p] = component(1, a, b);
   }
-  const auto pair = [D](int a, int b) {
-    if (a > b) std::swap(a, b);
-    return D == 2 ? (a == 0 ? b : 2) : (a == 0 ? b : (a == 1 ? 2 + b : 5));
-  };
-  for (int a = 0; a < D; ++a) nf[a].assign(static_cast<size_t>(N), T(0));
-  coh.assign(static_cast<size_t>(N), T(0));
-  for (int64_t i = 0; i < N; ++i) {
-    // the tensor in T: v = R1_a R1_c, then + h(a, k) h(k, c) for k = 0..D-1
-    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-    bool finite = true;
-    for (int a = 0; a < D; ++a) {
-      for (int c = a; c < D; ++c) {
-        T v = R1[a][i] * R1[c][i];
-        for (int k = 0; k < D; ++k) v = v + static_cast<T>(R2[pair(a, k)][i] * R2[pair(k, c)][i]);
-        A[a][c] = A[c][a] = static_cast<double>(v);
-        finite = finite && std::isfinite(A[a][c]);
-      }
-    }
-    if (!finite) nonfinite_ = true;
-    // Jacobi (element.cu:49-164): one rotation in 2-D; 6 cyclic sweeps after a power-of-two
-    // prescale in 3-D
-    const auto rotate = [&](int pp, int q, int rr, int dim) {
-      const double apq = A[pp][q];
-      if (apq == 0.0) return;
-      const double theta = (A[q][q] - A[pp][pp]) / (2.0 * apq);
-      const double at = std::fabs(theta);
-      const double t = std::copysign(1.0, theta) / (at + std::sqrt(theta * theta + 1.0));
-      const double cc = 1.0 / std::sqrt(t * t + 1.0);
-      const double s = t * cc;
-      const double tau = s / (1.0 + cc);
-      const double tapq = t * apq;
-      A[pp][pp] = A[pp][pp] - tapq;
-      A[q][q] = A[q][q] + tapq;
-      A[pp][q] = A[q][pp] = 0.0;
-      if (rr >= 0) {
-        const double gg = A[rr][pp], hh = A[rr][q];
-        const double np_ = gg - s * (hh + gg * tau);
-        const double nq_ = hh + s * (gg - hh * tau);
-        A[rr][pp] = A[pp][rr] = np_;
-        A[rr][q] = A[q][rr] = nq_;
-      }
-      for (int k = 0; k < dim; ++k) {
-        const double gg = V[k][pp], hh = V[k][q];
-        V[k][pp] = gg - s * (hh + gg * tau);
-        V[k][q] = hh + s * (gg - hh * tau);
-      }
-    };
-    if (D == 2) {
-      rotate(0, 1, -1, 2);
-    } else {
-      double am = 0.0;
-      for (int a = 0; a < 3; ++a) {
-        for (int c = a; c < 3; ++c) am = std::fmax(am, std::fabs(A[a][c]));
-      }
-      if (am > 0.0 && am < INFINITY) {
-        const double sc = std::scalbn(1.0, -std::ilogb(am));
-        for (int a = 0; a < 3; ++a) {
-          for (int c = 0; c < 3; ++c) A[a][c] = A[a][c] * sc;
-        }
-      }
-      for (int sweep = 0; sweep < 6; ++sweep) {
-        rotate(0, 1, 2, 3);
-        rotate(0, 2, 1, 3);
-        rotate(1, 2, 0, 3);
-      }
-    }
-    double mu[3] = {0.0, 0.0, 0.0};
-    for (int a = 0; a < D; ++a) mu[a] = A[a][a];
-    int top = 0;
-    for (int a = 1; a < D; ++a) top = mu[a] > mu[top] ? a : top;
-    double mu2 = -INFINITY;
-    for (int a = 0; a < D; ++a) mu2 = (a != top && mu[a] > mu2) ? mu[a] : mu2;
-    const double mu1 = mu[top];
-    const double ssum = mu1 + mu2;
-    double cv = ssum > 0.0 ? (mu1 - mu2) / ssum : 0.0;
-    cv = cv < 0.0 ? 0.0 : (cv > 1.0 ? 1.0 : cv);
-    coh[i] = static_cast<T>(cv);
-    for (int a = 0; a < D; ++a) nf[a][i] = static_cast<T>(V[a][top]);
-  }
+  bool nonfinite = false;
+  orientation_eigen<T>(D, N, R1, R2, nf, coh, &nonfinite);
+  if (nonfinite) nonfinite_ = true;
 }
 
 // d, e of a voxel (cpp/src/method/element.cuh:238-254)
@@ -1266,6 +1281,25 @@ Result Element<T>::run(const T* x, T* rows) {
         error = true;
         break;
       }
+      if (orient_) {
+        // the first component of magnitude above the dtype's default tie tolerance is positive
+        // (orientation.cu:412-418)
+        const T zero = static_cast<T>(std::is_same_v<T, float> ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
+        const int D = sh_.dim;
+        T* o = orient_ + static_cast<int64_t>(k_) * (D + 1) * N;
+        for (int64_t i = 0; i < N; ++i) {
+          int sgn = 0;
+          for (int a = 0; a < D; ++a) {
+            const T v = nv[a][static_cast<size_t>(i)];
+            if (sgn == 0 && std::fabs(v) > zero) sgn = v > T(0) ? 1 : -1;
+          }
+          for (int a = 0; a < D; ++a) {
+            const T v = nv[a][static_cast<size_t>(i)];
+            o[a * N + i] = sgn < 0 ? -v : v;
+          }
+          o[D * N + i] = coh[static_cast<size_t>(i)];
+        }
+      }
     }
     double d_min, d_max;
     element_build(L, coh, nv, &d_min, &d_max);
@@ -1415,6 +1449,162 @@ Ctl make_ctl(const Shape& sh, int32_t sifts) {
   return c;
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// eda.monogenic (cpp/src/method/monogenic.cpp:61-158; orientation.cu:420-493, 791-831): the
+// monogenic signal of one field, with the transforms as direct sums over the DCT bases in double.
+// Planes: amplitude, phase, frequency [count], then (D >= 2) direction [D][count] and coherence.
+template <class T>
+bool monogenic(const Shape& sh, const T* x, T* out) {
+  const int D = sh.dim;
+  const int64_t N = sh.count;
+  // the exact prescale f = x 2^-k, max|f| in [1, 2) (the driver's)
+  double amax = 0.0;
+  bool finite = true;
+  for (int64_t i = 0; i < N; ++i) {
+    const double v = static_cast<double>(x[i]);
+    if (!std::isfinite(v)) finite = false;
+    else amax = std::fmax(amax, std::fabs(v));
+  }
+  const int k = amax > 0.0 ? std::ilogb(amax) : 0;
+  std::vector<T> f(static_cast<size_t>(N));
+  for (int64_t i = 0; i < N; ++i) f[i] = static_cast<T>(std::ldexp(static_cast<double>(x[i]), -k));
+  double mean = 0.0;
+  for (int64_t i = 0; i < N; ++i) mean += static_cast<double>(f[i]);
+  mean = mean / static_cast<double>(N);
+  std::vector<double> X(static_cast<size_t>(N));
+  for (int64_t i = 0; i < N; ++i) X[i] = static_cast<double>(static_cast<T>(static_cast<double>(f[i]) - mean));
+  const auto axis_matrix = [](int64_t n, int kind) {
+    std::vector<double> m(static_cast<size_t>(n * n));
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int64_t i = 0; i < n; ++i) {
+      for (int64_t j = 0; j < n; ++j) {
+        const int64_t kk = kind == 0 ? i : j, xx = kind == 0 ? j : i;
+        const long double c = std::sqrt((kk ? 2.0L : 1.0L) / static_cast<long double>(n));
+        const int64_t q = (kk * (2 * xx + 1)) % (4 * n);
+        const long double ang = pi * static_cast<long double>(q) / static_cast<long double>(2 * n);
+        m[static_cast<size_t>(i * n + j)] = static_cast<double>(c * (kind == 2 ? std::sin(ang) : std::cos(ang)));
+      }
+    }
+    return m;
+  };
+  std::vector<double> M[kMaxDim][3];
+  for (int a = 0; a < D; ++a) {
+    for (int kk = 0; kk < 3; ++kk) M[a][kk] = axis_matrix(sh.n[a], kk);
+  }
+  const auto apply_axis = [&](int a, const std::vector<double>& m, std::vector<double>& g) {
+    const int64_t n = sh.n[a], st = sh.st[a];
+    std::vector<double> line(static_cast<size_t>(n));
+    for (int64_t l = 0; l < sh.lines(a); ++l) {
+      const int64_t base = sh.line_base(a, l);
+      for (int64_t i = 0; i < n; ++i) line[i] = g[base + i * st];
+      for (int64_t i = 0; i < n; ++i) {
+        double acc = 0.0;
+        const double* row = &m[static_cast<size_t>(i * n)];
+        for (int64_t j = 0; j < n; ++j) acc += row[j] * line[j];
+        g[base + i * st] = acc;
+      }
+    }
+  };
+  for (int a = 0; a < D; ++a) apply_axis(a, M[a][0], X);
+  std::vector<double> uk(static_cast<size_t>(D * N)), rad(static_cast<size_t>(N));
+  for (int64_t i = 0; i < N; ++i) {
+    int32_t kk[kMaxDim];
+    sh.coords(i, kk);
+    double r2 = 0.0;
+    for (int a = 0; a < D; ++a) {
+      const double u = static_cast<double>(kk[a]) * (1.0 / (2.0 * static_cast<double>(sh.n[a])));
+      uk[a * N + i] = u;
+      r2 = r2 + u * u;
+    }
+    rad[i] = std::sqrt(r2);
+    X[i] = static_cast<double>(static_cast<T>(X[i]));  // the spectrum is held in T
+  }
+  // kinds (riesz_mult, orientation.cu:116-127): 0 R1_a, 1 R2_aa, 2 R2_ab, 3 D_a f, 4 D_b R_a
+  const auto component = [&](int kind, int a, int b) {
+    std::vector<double> y(static_cast<size_t>(N), 0.0);
+    for (int64_t i = 0; i < N; ++i) {
+      if (!(rad[i] > 0.0)) continue;
+      const double inv = 1.0 / rad[i];
+      const double ua = uk[a * N + i] * inv;
+      double m;
+      if (kind == 0) m = ua;
+      else if (kind == 1) m = -ua * ua;
+      else if (kind == 3) m = -uk[a * N + i];
+      else if (kind == 4) m = a == b ? uk[a * N + i] * ua : -(uk[a * N + i] * (uk[b * N + i] * inv));
+      else m = ua * (uk[b * N + i] * inv);
+      y[i] = static_cast<double>(static_cast<T>(m * X[i]));
+    }
+    const int odd = (kind == 0 || kind == 3) ? (1 << a) : (a == b ? 0 : ((1 << a) | (1 << b)));
+    for (int ax = 0; ax < D; ++ax) apply_axis(ax, M[ax][((odd >> ax) & 1) ? 2 : 1], y);
+    std::vector<T> o(static_cast<size_t>(N));
+    for (int64_t i = 0; i < N; ++i) o[i] = static_cast<T>(y[i]);
+    return o;
+  };
+  std::vector<T> R1[kMaxDim], DF[kMaxDim], R2[6], DR[6];
+  for (int a = 0; a < D; ++a) {
+    R1[a] = component(0, a, a);
+    DF[a] = component(3, a, a);
+  }
+  int np = 0;
+  for (int a = 0; a < D; ++a) {
+    for (int b = a; b < D; ++b, ++np) {
+      if (D >= 2) R2[np] = component(a == b ? 1 : 2, a, b);
+      DR[np] = component(4, a, b);
+    }
+  }
+  std::vector<T> nv[kMaxDim], coh;
+  if (D >= 2) {
+    bool eig_nonfinite = false;
+    orientation_eigen<T>(D, N, R1, R2, nv, coh, &eig_nonfinite);
+  }
+  const T zero = static_cast<T>(std::is_same_v<T, float> ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
+  const double tiny = std::is_same_v<T, float> ? static_cast<double>(FLT_MIN) : 1e-300;
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int64_t i = 0; i < N; ++i) {
+    T nt[kMaxDim] = {T(1), T(0), T(0)};
+    if (D >= 2) {
+      int s = 0;
+      for (int a = 0; a < D; ++a) {
+        nt[a] = nv[a][static_cast<size_t>(i)];
+        if (s == 0 && std::fabs(nt[a]) > zero) s = nt[a] > T(0) ? 1 : -1;
+      }
+      for (int a = 0; a < D; ++a) nt[a] = s < 0 ? -nt[a] : nt[a];
+    }
+    const double fv = static_cast<double>(f[i]);
+    double q = 0.0, a2 = fv * fv, dnf = 0.0, dnq = 0.0;
+    for (int a = 0; a < D; ++a) {
+      const double r = static_cast<double>(R1[a][i]);
+      const double na = static_cast<double>(nt[a]);
+      q = q + na * r;
+      a2 = a2 + r * r;
+      dnf = dnf + na * static_cast<double>(DF[a][i]);
+    }
+    int p = 0;
+    for (int a = 0; a < D; ++a) {
+      for (int c = a; c < D; ++c, ++p) {
+        const double na = static_cast<double>(nt[a]), nc = static_cast<double>(nt[c]);
+        const double m = a == c ? na * na : 2.0 * (na * nc);
+        dnq = dnq + m * static_cast<double>(DR[p][i]);
+      }
+    }
+    double phase = 0.0, freq = 0.0;
+    if (a2 > tiny) {
+      phase = std::atan2(q, fv);
+      freq = (fv * dnq - q * dnf) / a2;
+    }
+    out[i] = static_cast<T>(std::ldexp(std::sqrt(a2), k));
+    const T pt = static_cast<T>(phase);
+    out[N + i] = pt == -static_cast<T>(pi) ? static_cast<T>(pi) : pt;
+    out[2 * N + i] = static_cast<T>(freq);
+    if (D >= 2) {
+      for (int a = 0; a < D; ++a) out[(3 + a) * N + i] = nt[a];
+      out[(3 + D) * N + i] = coh[static_cast<size_t>(i)];
+    }
+  }
+  return finite;
+}
+
 }  // namespace oracle
 
 // ---------------------------------------------------------------------------------------------
@@ -1431,10 +1621,28 @@ int eda_oracle_rows_cap(int dim, const int64_t* n, int32_t max_imf) {
   return modes_max + 2;
 }
 
+int eda_oracle_decompose_orientation(const void* x, int dtype, int dim, int64_t batch, const int64_t* n,
+                                     int32_t max_imf, double tie, int32_t sifts, int32_t check_finite, int32_t threads,
+                                     void* rows, int32_t* n_imfs, int32_t* error, int32_t* windows,
+                                     int32_t* sifts_out, double* spacing, double* energy, int32_t* exps,
+                                     void* orient, char* err, int64_t err_len);
+
 int eda_oracle_decompose(const void* x, int dtype, int dim, int64_t batch, const int64_t* n, int32_t max_imf,
                          double tie, int32_t sifts, int32_t check_finite, int32_t threads, void* rows,
                          int32_t* n_imfs, int32_t* error, int32_t* windows, int32_t* sifts_out, double* spacing,
                          double* energy, int32_t* exps, char* err, int64_t err_len) {
+  return eda_oracle_decompose_orientation(x, dtype, dim, batch, n, max_imf, tie, sifts, check_finite, threads, rows,
+                                          n_imfs, error, windows, sifts_out, spacing, energy, exps, nullptr, err,
+                                          err_len);
+}
+
+// eda_oracle_decompose that also keeps the orientation rows (B, cap - 1, D + 1, count) in orient
+// (zero where no mode ran); orient NULL keeps none.
+int eda_oracle_decompose_orientation(const void* x, int dtype, int dim, int64_t batch, const int64_t* n,
+                                     int32_t max_imf, double tie, int32_t sifts, int32_t check_finite, int32_t threads,
+                                     void* rows, int32_t* n_imfs, int32_t* error, int32_t* windows,
+                                     int32_t* sifts_out, double* spacing, double* energy, int32_t* exps,
+                                     void* orient, char* err, int64_t err_len) {
   try {
     const oracle::Shape sh(dim, n);
     const int32_t cap = eda_oracle_rows_cap(dim, n, max_imf);
@@ -1446,6 +1654,11 @@ int eda_oracle_decompose(const void* x, int dtype, int dim, int64_t batch, const
         oracle::Ctl c = oracle::make_ctl<T>(sh, sifts);
         const double tau = tie >= 0 ? tie : (std::is_same_v<T, float> ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
         oracle::Element<T> el(sh, c, tau, check_finite != 0, max_imf, cap);
+        if (orient && dim >= 2) {
+          T* o = static_cast<T*>(orient) + b * (cap - 1) * (dim + 1) * N;
+          std::fill(o, o + (cap - 1) * (dim + 1) * N, T(0));
+          el.keep_orientation(o);
+        }
         T* out = static_cast<T*>(rows) + b * cap * N;
         std::fill(out, out + cap * N, T(0));
         const oracle::Result r = el.run(static_cast<const T*>(x) + b * N, out);
@@ -1493,6 +1706,36 @@ int eda_oracle_decompose(const void* x, int dtype, int dim, int64_t batch, const
       std::strncpy(err, e.what(), static_cast<size_t>(err_len - 1));
       err[err_len - 1] = 0;
     }
+    return -1;
+  }
+}
+
+// eda.monogenic of batch fields of x (batch, n..): out (3 [+ D + 1 in 2-D / 3-D]) planes of
+// batch x count in the reference's native layout (amplitude, phase, frequency, direction
+// [batch][D][count], coherence); nonfinite[b] = 1 where field b holds inf or NaN.
+int eda_oracle_monogenic(const void* x, int dtype, int dim, int64_t batch, const int64_t* n, void* out,
+                         int32_t* nonfinite) {
+  try {
+    const oracle::Shape sh(dim, n);
+    const int64_t N = sh.count;
+    const int planes = dim == 1 ? 3 : 4 + dim;
+    const auto body = [&](auto tag) {
+      using T = decltype(tag);
+      std::vector<T> one(static_cast<size_t>(planes * N));
+      for (int64_t b = 0; b < batch; ++b) {
+        nonfinite[b] = oracle::monogenic<T>(sh, static_cast<const T*>(x) + b * N, one.data()) ? 0 : 1;
+        T* o = static_cast<T*>(out);
+        for (int pl = 0; pl < 3; ++pl) std::copy(one.begin() + pl * N, one.begin() + (pl + 1) * N, o + (pl * batch + b) * N);
+        if (dim >= 2) {
+          std::copy(one.begin() + 3 * N, one.begin() + (3 + dim) * N, o + 3 * batch * N + b * dim * N);
+          std::copy(one.begin() + (3 + dim) * N, one.begin() + (4 + dim) * N, o + (3 + dim) * batch * N + b * N);
+        }
+      }
+    };
+    if (dtype == 0) body(float{});
+    else body(double{});
+    return 0;
+  } catch (...) {
     return -1;
   }
 }

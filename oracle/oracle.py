@@ -48,6 +48,15 @@ def lib() -> ctypes.CDLL:
             i32p, i32p, i32p, i32p, f64p, f64p, i32p, ctypes.c_char_p, ctypes.c_int64,
         ]
         L.eda_oracle_decompose.restype = ctypes.c_int
+        L.eda_oracle_decompose_orientation.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64, i64p, ctypes.c_int32,
+            ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+            i32p, i32p, i32p, i32p, f64p, f64p, i32p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64,
+        ]
+        L.eda_oracle_decompose_orientation.restype = ctypes.c_int
+        L.eda_oracle_monogenic.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64, i64p,
+                                           ctypes.c_void_p, i32p]
+        L.eda_oracle_monogenic.restype = ctypes.c_int
         L.eda_oracle_rung_ladder.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, i32p]
         L.eda_oracle_rung_ladder.restype = ctypes.c_int
         L.eda_oracle_cube.argtypes = [ctypes.c_int, ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int32, ctypes.c_void_p]
@@ -66,8 +75,9 @@ def rows_cap(shape: tuple[int, ...], max_imf: int = -1) -> int:
 
 
 def decompose_raw(x: np.ndarray, max_imf: int = -1, tie_tolerance: float | None = None, sifts: int = 3,
-                  check_finite: bool = True, threads: int = 1) -> tuple[np.ndarray, dict]:
-    """The oracle on (B, *spatial): rows (B, cap, *spatial) and the raw per-element arrays."""
+                  check_finite: bool = True, threads: int = 1, orientation: bool = False) -> tuple[np.ndarray, dict]:
+    """The oracle on (B, *spatial): rows (B, cap, *spatial) and the raw per-element arrays; with
+    ``orientation`` also ``orient`` (B, cap - 1, D + 1, *spatial): n (canonical sign) and c per mode."""
     x = np.ascontiguousarray(x)
     assert x.dtype in (np.float32, np.float64) and 2 <= x.ndim <= 4
     B, spatial = x.shape[0], x.shape[1:]
@@ -83,16 +93,20 @@ def decompose_raw(x: np.ndarray, max_imf: int = -1, tie_tolerance: float | None 
     spacing = np.zeros((B, he), np.float64)
     energy = np.zeros((B, he), np.float64)
     err = ctypes.create_string_buffer(512)
-    rc = lib().eda_oracle_decompose(
+    orient = np.zeros((B, he, len(spatial) + 1) + spatial, dtype=x.dtype) if orientation else None
+    rc = lib().eda_oracle_decompose_orientation(
         x.ctypes.data, 0 if x.dtype == np.float32 else 1, len(spatial), B, _p(n, ctypes.c_int64), max_imf,
         -1.0 if tie_tolerance is None else float(tie_tolerance), sifts, int(bool(check_finite)), threads,
         rows.ctypes.data, _p(n_imfs, ctypes.c_int32), _p(error, ctypes.c_int32), _p(windows, ctypes.c_int32),
         _p(sifts_out, ctypes.c_int32), _p(spacing, ctypes.c_double), _p(energy, ctypes.c_double),
-        _p(exps, ctypes.c_int32), err, 512)
+        _p(exps, ctypes.c_int32), None if orient is None else orient.ctypes.data, err, 512)
     if rc != 0:
         raise RuntimeError(f"oracle: {err.value.decode()}")
-    return rows, {"n_imfs": n_imfs, "error": error, "windows": windows, "sifts": sifts_out,
-                  "spacing": spacing, "energy": energy, "exp": exps}
+    out = {"n_imfs": n_imfs, "error": error, "windows": windows, "sifts": sifts_out,
+           "spacing": spacing, "energy": energy, "exp": exps}
+    if orient is not None:
+        out["orient"] = orient
+    return rows, out
 
 
 def decompose(x: np.ndarray, max_imf: int = -1, tie_tolerance: float | None = None, sifts: int = 3,
@@ -110,6 +124,24 @@ def decompose(x: np.ndarray, max_imf: int = -1, tie_tolerance: float | None = No
         info[name] = a
     out = rows[:, :P].copy()
     return out, info
+
+
+def monogenic(x: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The monogenic signal of the fields of x (B, *spatial): the native planes (amplitude, phase,
+    frequency (B, count) each, then in 2-D / 3-D direction (B, D, count) and coherence (B, count)),
+    flattened, and the non-finite flags [B]."""
+    x = np.ascontiguousarray(x)
+    B, spatial = x.shape[0], x.shape[1:]
+    D = len(spatial)
+    count = int(np.prod(spatial))
+    planes = 3 if D == 1 else 4 + D
+    out = np.zeros(planes * B * count, dtype=x.dtype)
+    bad = np.zeros(B, np.int32)
+    n = np.asarray(spatial, dtype=np.int64)
+    if lib().eda_oracle_monogenic(x.ctypes.data, 0 if x.dtype == np.float32 else 1, D, B, _p(n, ctypes.c_int64),
+                                  out.ctypes.data, _p(bad, ctypes.c_int32)) != 0:
+        raise RuntimeError("oracle: monogenic")
+    return out, bad
 
 
 def rung_ladder(d_min: float, d_max: float, w: int, n_max: int) -> list[int]:

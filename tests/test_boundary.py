@@ -96,3 +96,24 @@ def test_empty_batch_computes_nothing():
 
     y, info = eda.decompose(np.zeros((0, 8), np.float32), axes=1, return_info=True)
     assert y.shape == (0, 1, 8) and info.windows.shape == (0, 0)
+
+
+@pytest.mark.parametrize("xs,exc", [
+    (np.zeros(10), TypeError),
+    ([np.zeros(10), np.zeros((4, 4))], ValueError),
+    ([np.zeros(10, np.float32), np.zeros(12, np.float64)], TypeError),
+    ([np.zeros(10, np.int32)], TypeError),
+    ([np.zeros((2, 2, 2, 2))], ValueError),
+])
+def test_ragged_argument_rules(xs, exc):
+    import eda
+
+    with pytest.raises(exc):
+        eda.decompose_ragged(xs)
+
+
+def test_ragged_empty_batch():
+    import eda
+
+    assert eda.decompose_ragged([]) == []
+    assert eda.decompose_ragged([], return_info=True) == ([], [])

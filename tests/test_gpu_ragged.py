@@ -1,0 +1,121 @@
+# SPDX-License-Identifier: Apache-2.0
+"""Ragged batches (eda.decompose_ragged / eda_decompose_ragged): fields of different shapes in one
+call. Every field's rows and information must equal, bit for bit, what eda.decompose gives for it
+alone (the reference's way to run a ragged workload: one call per shape), whatever the grouping,
+the order of the fields and the number of concurrent workers."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    t = pytest.importorskip("torch")
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+def signal(n: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    t = np.arange(n, dtype=np.float64)
+    f0 = rng.uniform(0.002, 0.01)
+    return (np.cos(2 * np.pi * (f0 * t + 0.5 * (0.2 - f0) / n * t * t)) + 0.8 * np.cos(rng.uniform(0.05, 0.3) * t)
+            + rng.uniform(-1e-3, 1e-3) * t + 0.01 * rng.standard_normal(n))
+
+
+def image(h: int, w: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:h, 0:w].astype(np.float64)
+    cy, cx = rng.uniform(0, h), rng.uniform(0, w)
+    return (np.cos(2 * np.pi * np.hypot(y - cy, x - cx) / 6) + 1.5 * np.cos(2 * np.pi * x / 24)
+            + 3 * np.exp(-((y - h / 2) ** 2 + (x - w / 3) ** 2) / (2 * (h / 4) ** 2)) + 0.02 * rng.standard_normal((h, w)))
+
+
+def alone(eda, x: np.ndarray):
+    rows, info = eda.decompose(x[None], axes=tuple(range(1, x.ndim + 1)), return_info=True, errors="status")
+    k = int(info.n_imfs[0]) if int(info.error[0]) == 0 else 0
+    return rows[0, : (k + 1 if int(info.error[0]) == 0 else 1)], info, k
+
+
+def same(a: np.ndarray, b: np.ndarray) -> bool:
+    u = np.uint32 if a.dtype == np.float32 else np.uint64
+    return a.shape == b.shape and np.array_equal(np.ascontiguousarray(a).view(u), np.ascontiguousarray(b).view(u))
+
+
+def check_against_alone(eda, xs, rows, infos):
+    assert len(rows) == len(xs) == len(infos)
+    for i, x in enumerate(xs):
+        want, winfo, k = alone(eda, x)
+        assert same(np.asarray(rows[i]), np.asarray(want)), i
+        assert int(infos[i].n_imfs) == int(winfo.n_imfs[0]) and int(infos[i].error) == int(winfo.error[0])
+        np.testing.assert_array_equal(infos[i].windows, winfo.windows[0, :k])
+        np.testing.assert_array_equal(infos[i].sifts, winfo.sifts[0, :k])
+        np.testing.assert_array_equal(infos[i].spacing, winfo.spacing[0, :k])
+        np.testing.assert_array_equal(infos[i].energy, winfo.energy[0, :k])
+
+
+def test_ragged_1d_equals_one_call_per_field(torch):
+    import eda
+
+    lengths = [300, 2048, 511, 1024, 300, 777, 4096, 1024, 2, 300, 6000, 513]
+    xs = [signal(n, 7 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    rows, infos = eda.decompose_ragged(xs, return_info=True)
+    check_against_alone(eda, xs, rows, infos)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_ragged_2d_equals_one_call_per_field(torch, dtype):
+    import eda
+
+    shapes = [(40, 56), (64, 64), (40, 56), (33, 90), (64, 64), (96, 128), (40, 56)]
+    xs = [image(h, w, 3 + i).astype(dtype) for i, (h, w) in enumerate(shapes)]
+    rows, infos = eda.decompose_ragged(xs, return_info=True)
+    check_against_alone(eda, xs, rows, infos)
+
+
+def test_ragged_results_do_not_depend_on_the_workers(torch):
+    import eda
+
+    lengths = [700, 900, 700, 1500, 900, 64, 3000]
+    xs = [signal(n, 100 + i) for i, n in enumerate(lengths)]
+    one = eda.decompose_ragged(xs, workers=1)
+    many = eda.decompose_ragged(xs, workers=8)
+    for a, b in zip(one, many):
+        assert same(a, b)
+
+
+def test_ragged_device_input(torch):
+    import eda
+
+    lengths = [500, 1200, 500, 2500]
+    xs = [signal(n, 40 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    xd = [torch.from_numpy(x).cuda() for x in xs]
+    rows = eda.decompose_ragged(xd)
+    host = eda.decompose_ragged(xs)
+    for r, h in zip(rows, host):
+        assert same(r.cpu().numpy() if hasattr(r, "cpu") else np.asarray(r), h)
+
+
+def test_ragged_failed_field(torch):
+    import eda
+
+    xs = [signal(400, 1), signal(500, 2), signal(400, 3)]
+    xs[1][17] = np.nan
+    with pytest.raises(eda.DecompositionError) as e:
+        eda.decompose_ragged(xs)
+    assert list(e.value.indices) == [1]
+    rows, infos = eda.decompose_ragged(xs, errors="status", return_info=True)
+    assert rows[1].shape == (1, 500) and np.isnan(rows[1]).all() and int(infos[1].error) == 1
+    check_against_alone(eda, [xs[0], xs[2]], [rows[0], rows[2]], [infos[0], infos[2]])
+
+
+def test_ragged_rejects_a_field_beyond_the_axis_limit(torch):
+    import eda
+
+    with pytest.raises(ValueError, match="exceeds the limit"):
+        eda.decompose_ragged([signal(300, 1).astype(np.float32), signal(8193, 2).astype(np.float32)])
