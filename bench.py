@@ -393,6 +393,28 @@ def run_other(args) -> None:
 import ctypes  # noqa: E402
 
 
+def write_traffic(csv_path: Path) -> None:
+    """Sums dram__bytes_read.sum + dram__bytes_write.sum over the cube-pass launches of an ncu CSV
+    log (one row per metric and launch) into the per-launch DRAM traffic the roofline reports."""
+    import csv
+
+    rows = list(csv.reader(csv_path.open()))
+    h = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    hdr = rows[h]
+    ki, mi, vi, ui, ii = (hdr.index(k) for k in ("Kernel Name", "Metric Name", "Metric Value", "Metric Unit", "ID"))
+    scale = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    per: dict[str, float] = {}
+    for r in rows[h + 1:]:
+        if "cube_pass" in r[ki] and r[mi] in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            per[r[ii]] = per.get(r[ii], 0.0) + float(r[vi].replace(",", "")) * scale[r[ui]]
+    if not per:
+        raise SystemExit(f"{csv_path}: no cube_pass DRAM metrics")
+    out = {"kernel": "cube_pass", "launches": len(per), "dram_bytes": sum(per.values()),
+           "dram_bytes_per_launch": sum(per.values()) / len(per)}
+    TRAFFIC.write_text(json.dumps(out, indent=1) + "\n")
+    print(json.dumps(out))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -405,8 +427,13 @@ def main() -> None:
                     help="images per GPU of the 2-D benchmark (64; smaller only for profiling captures)")
     ap.add_argument("--workload", default="2d", choices=("2d", "1d", "3d", "ragged1d", "ragged2d"),
                     help="2d: the benchmark (default); the others measure the remaining configurations on 1 GPU")
+    ap.add_argument("--traffic-from", metavar="CSV",
+                    help="write the cube passes' DRAM bytes per launch from an ncu --csv log of "
+                         "dram__bytes_read.sum and dram__bytes_write.sum to profiles/ and exit")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.traffic_from:
+        write_traffic(Path(args.traffic_from))
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload != "2d":
         run_other(args)

@@ -12,18 +12,22 @@
 // Box sums run axis 0 first and the last pass multiplies by fl_T(1 / prod of the clamped sides);
 // max and min fold the integer order keys of the values (the order of max_c / min_c).
 //
-// B200 design. A CTA stages P lines of one element (rows of the contiguous axis, or a panel of P
-// adjacent columns of an outer axis: whole 32-byte sectors) in shared memory, interleaved: sample i
-// of line p at i * PP + p. Lanes map to lines: P lanes of a warp ("a worker") run the same fold
-// task on their P lines, so control flow is uniform and a worker's shared-memory accesses are
-// consecutive words. The fold tasks (one per direction, segment and 32-sample chunk) are spread over
-// the CTA's workers: chunk totals, per-segment exclusive carries, then the H folds and the G folds
-// combined with them. P is a compile-time constant, so a whole 32-sample chunk inside the line runs
+// B200 design. A CTA runs a run of consecutive line groups of one element (and one rung, or every
+// rung of a ladder that shares its input); a group is P lines: P rows of the contiguous axis, or a
+// panel of P adjacent columns of an outer axis. Shared-memory layouts keep every global transfer a
+// 16-byte copy: rows are stored line after line with a padded line stride (4 words modulo 32, so
+// the P lanes of a worker reading one sample of P lines hit distinct banks); a column panel keeps
+// its global row layout, sample i of line p at i P + p. The next group's input is copied with
+// cp.async into the second of two buffers while the current group is folded; order keys (max /
+// min) are formed in place by the threads that copied the samples. The window setup of every rung
+// is made once per CTA. Lanes map to lines: P lanes of a warp ("a worker") run the same fold task
+// on their P lines, so control flow is uniform. The fold tasks (one per direction, segment and
+// 32-sample chunk) are spread over the CTA's workers: chunk totals, per-segment exclusive carries,
+// then the H folds and the G folds combined with them. A whole 32-sample chunk inside the line runs
 // as an unrolled fold with immediate shared-memory offsets; only the chunks that cross a line end,
 // the window's first r samples or a segment end take the general path. A chunk without a carry
 // folds from the operation's identity (-0 for sums, the extreme keys for max / min), which changes
-// no bit of any result. The first pass of a cube stages its input once and runs every rung of the
-// ladder on it (the operators' rung group); later passes run one rung per CTA.
+// no bit of any result.
 #include "engine.cuh"
 
 #include <algorithm>
@@ -35,12 +39,27 @@ namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
 constexpr int kWarps = kThreads / 32;
-constexpr int kStageLoads = 8;  // global loads in flight per thread while staging lines
+constexpr int kMaxGroupsPerCta = 8;  // line groups one CTA runs at most
 
 __host__ __device__ constexpr int32_t tot_slots(int32_t n) { return n / 8 + 24; }
-// Words per staged sample row: P lines plus one (odd, so a transposed row staging of 32
-// consecutive samples hits 32 distinct banks); one line is stored contiguously.
-__host__ __device__ constexpr int32_t line_pitch(int P) { return P == 1 ? 1 : P + 1; }
+// Line stride of the row layout in elements: the padded row rounded up, plus 16 bytes (4 words
+// modulo 32 for 4-byte samples, 2 elements modulo 16 for 8-byte samples).
+template <class T>
+__host__ __device__ constexpr int32_t row_stride(int32_t n) {
+  return sizeof(T) == 4 ? ((n + 31) & ~31) + 4 : ((n + 15) & ~15) + 2;
+}
+// Elements of one line-group buffer (a multiple of 16 bytes).
+template <class T>
+__host__ __device__ constexpr int32_t group_elems(int32_t n, int P, bool rows) {
+  return rows ? P * row_stride<T>(n) : ((n * P + 3) & ~3);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Order key of v as a T-sized integer (its own inverse): integer order = order of max_c/min_c.
 __device__ __forceinline__ float okey(float v) {
@@ -279,8 +298,19 @@ __device__ __forceinline__ void partial_g(const T* __restrict__ v, T* __restrict
 // samples apart, spreading their shared-memory banks). Advanced without divisions.
 struct Tasks {
   int32_t k, c, dk, dc;
-  __device__ __forceinline__ Tasks(int32_t first, int32_t stride, int32_t nseg)
-      : k(first % nseg), c(first / nseg), dk(stride % nseg), dc(stride / nseg) {}
+  __device__ __forceinline__ Tasks(int32_t first, int32_t stride, int32_t nseg) {
+    if (nseg > stride) {  // first < stride: no division
+      k = first;
+      c = 0;
+      dk = stride;
+      dc = 0;
+    } else {
+      k = first % nseg;
+      c = first / nseg;
+      dk = stride % nseg;
+      dc = stride / nseg;
+    }
+  }
   __device__ __forceinline__ void next(int32_t nseg) {
     k += dk;
     c += dc;
@@ -291,20 +321,19 @@ struct Tasks {
   }
 };
 
-// One stage on the staged lines of this CTA: V -> R (both n x PP, line p at column p), tot: the
-// chunk totals / carries [2][TS][PP] (slot k cps + c). Workers: P lanes each (lane % P = the line).
-template <class T, int OP, int P>
+// One stage on the staged lines of this CTA: V -> R (sample i of line p at p LS + i PP), tot: the
+// chunk totals / carries [2][TS][P] (slot k cps + c). Workers: P lanes each (lane % P = the line).
+template <class T, int OP, int P, int PP>
 __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int32_t n,
-                                          int32_t TS, const Win& q) {
-  constexpr int PP = line_pitch(P);
+                                          int32_t TS, const Win& q, int32_t LS) {
   constexpr int slots = 32 / P;
   constexpr int workers = kWarps * slots;
   const int lane = threadIdx.x & 31;
   const int p = lane & (P - 1);
   const int worker = (threadIdx.x >> 5) * slots + lane / P;
   const int32_t e_max = n - 1 + q.r;
-  const T* Vp = V + p;
-  T* Rp = R + p;
+  const T* Vp = V + p * LS;
+  T* Rp = R + p * LS;
   const T idn = fold_identity<T, OP>();
   if (q.cps > 1) {
     // phase 1: chunk totals; half of the workers take the line, half the reversed line
@@ -328,7 +357,7 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
       } else {
         total = fold_chunk<T, OP>(Vp, PP, n, c0, c1, dir, [](int32_t, T) {});
       }
-      tot[(dir * TS + t.k * q.cps + t.c) * PP + p] = total;
+      tot[(dir * TS + t.k * q.cps + t.c) * P + p] = total;
     }
     __syncthreads();
     // phase 2: exclusive carries per segment, in place (slot c holds the carry of chunk c >= 1)
@@ -338,11 +367,11 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t nch = (e_last - s) / 32 + 1;
-      T* tl = tot + (dir * TS + k * q.cps) * PP + p;
+      T* tl = tot + (dir * TS + k * q.cps) * P + p;
       T run = tl[0];
       for (int32_t c = 1; c < nch; ++c) {
-        const T next = tl[c * PP];
-        tl[c * PP] = run;
+        const T next = tl[c * P];
+        tl[c * P] = run;
         run = fop<OP>(run, next);
       }
     }
@@ -355,7 +384,7 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     const int32_t c0 = s + 32 * t.c;
     if (c0 > e_last) continue;
     const int32_t c1 = min(c0 + 31, e_last);
-    const T cv = t.c > 0 ? tot[(TS + t.k * q.cps + t.c) * PP + p] : idn;
+    const T cv = t.c > 0 ? tot[(TS + t.k * q.cps + t.c) * P + p] : idn;
     if (c0 >= 0 && c1 <= n - 1) {
       const T* vp = Vp + (n - 1 - c0) * PP;
       T* rp = Rp + (n - 1 + q.r - c0) * PP;  // the slot of e = c0 (written only when c0 >= r)
@@ -376,7 +405,7 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     const int32_t c0 = s + 32 * t.c;
     if (c0 > e_last) continue;
     const int32_t c1 = min(c0 + 31, e_last);
-    const T cv = t.c > 0 ? tot[(t.k * q.cps + t.c) * PP + p] : idn;
+    const T cv = t.c > 0 ? tot[(t.k * q.cps + t.c) * P + p] : idn;
     if (c0 >= 0 && c1 <= n - 1) {
       const T* vp = Vp + c0 * PP;
       T* rp = Rp + (c0 - q.r) * PP;  // the slot of e = c0 (written only when c0 >= r)
@@ -418,177 +447,350 @@ struct PassArgs {
   int32_t epi;            // BoxEpi on the last pass
   const T* aux;
   int32_t rung_loop;      // 1: the CTA loops over the rungs (shared input); else blockIdx.z is the rung
+  int32_t vec;            // every pointer and stride allows 16-byte copies
+  int64_t groups;         // line groups per element
+  int32_t gpc;            // line groups per CTA (blockIdx.x runs groups [x gpc, x gpc + gpc))
   unsigned long long* bytes;  // instrumentation: the pass's algorithmic bytes (nullptr: off)
 };
 
-// Thread roles of the staging and the store of P lines of n samples. Rows (the contiguous axis):
-// warps take lines (kWarps / P warps per line when P < kWarps), lanes consecutive samples. Column
-// panels: thread t takes line t % P and samples t / P + k kThreads / P.
-template <int P>
-struct LineRoles {
-  static constexpr int kWpl = P >= kWarps ? 1 : kWarps / P;  // warps per line (rows)
-  static constexpr int kRowStride = 32 * kWpl;                 // sample stride of a thread (rows)
-  static constexpr int kColStride = kThreads / P;              // sample stride of a thread (columns)
+// Where a line group lies inside its element: rows, line p at base + p pitch; column panels, line
+// p at base + p (rows of the panel `step` apart). mask: bit p set for a line of the field (rows
+// inside the element, columns left of the row padding).
+struct GroupPos {
+  int64_t base;
+  uint32_t mask;
+  int32_t o, c, cpos;  // rows: c is the first row; column panels: outer index, first column, first
+                       // column modulo the pitch
+};
+template <int P, bool ROWS>
+__device__ __forceinline__ GroupPos group_at(const Geom& g, int64_t grp, int32_t n, int64_t inner) {
+  GroupPos s{};
+  if constexpr (ROWS) {
+    s.c = static_cast<int32_t>(grp * P);
+  } else {
+    // 32-bit divisions (an element holds fewer than 2^31 samples)
+    const uint32_t gpo = static_cast<uint32_t>(inner) / P;
+    s.o = static_cast<int32_t>(static_cast<uint32_t>(grp) / gpo);
+    s.c = static_cast<int32_t>((static_cast<uint32_t>(grp) - static_cast<uint32_t>(s.o) * gpo) * P);
+    s.cpos = static_cast<int32_t>(static_cast<uint32_t>(s.c) % static_cast<uint32_t>(g.pitch));
+  }
+  return s;
+}
+template <int P, bool ROWS>
+__device__ __forceinline__ void group_next(GroupPos& s, const Geom& g, int32_t n, int64_t inner) {
+  if constexpr (ROWS) {
+    s.c += P;
+  } else {
+    s.c += P;
+    s.cpos += P;
+    if (s.cpos == g.pitch) s.cpos = 0;
+    if (s.c == inner) {
+      s.c = 0;
+      ++s.o;
+    }
+  }
+}
+template <int P, bool ROWS>
+__device__ __forceinline__ void group_finish(GroupPos& s, const Geom& g, int32_t n, int64_t inner) {
+  if constexpr (ROWS) {
+    s.base = static_cast<int64_t>(s.c) * g.pitch;
+    const int64_t left = g.rows - s.c;
+    s.mask = left >= P ? (1u << P) - 1u : (left > 0 ? (1u << left) - 1u : 0u);
+  } else {
+    s.base = static_cast<int64_t>(s.o) * n * inner + s.c;
+    const int32_t room = g.n_last - s.cpos;  // columns of the panel left of the padding
+    s.mask = room >= P ? (1u << P) - 1u : (room > 0 ? (1u << room) - 1u : 0u);
+  }
+}
+
+template <class T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
 };
 
-template <class T, int P>
-__global__ void __launch_bounds__(kThreads, 5) cube_pass(Geom g, PassArgs<T> a) {
-  constexpr int PP = line_pitch(P);
-  using Roles = LineRoles<P>;
+template <class T, int P, bool ROWS>
+__global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) {
+  constexpr int VW = 16 / static_cast<int>(sizeof(T));  // samples per 16-byte copy
+  constexpr int PP = ROWS ? 1 : P;                        // sample stride in shared memory
+  using V16 = typename Vec16<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ Win win_s[kMaxRungs];
+  __shared__ T fac_s[kMaxRungs];
+  __shared__ int32_t any_s;
   const int64_t b = blockIdx.y;
   const int axis = a.axis;
   // (a kernel parameter indexed by a runtime value would be copied to local memory)
   const int32_t n = geom_n(g, axis);
-  const int64_t axis_stride = geom_stride(g, axis);
-  const int32_t n_last = geom_n(g, g.dim - 1);
-  const bool contig = axis == g.dim - 1;
+  const int64_t inner = ROWS ? 1 : geom_stride(g, axis);  // column panels: the axis stride
+  const int64_t step = ROWS ? 1 : inner;
   const int32_t TS = tot_slots(n);
-  T* V = reinterpret_cast<T*>(smem_raw);
-  T* R = V + static_cast<int64_t>(n) * PP;
-  T* tot = R + static_cast<int64_t>(n) * PP;
-  __shared__ int64_t base_s[32];
-  __shared__ int32_t ok_s[32];
-  const int64_t grp = blockIdx.x;
-  if (threadIdx.x < P) {
-    const int p = threadIdx.x;
-    bool ok;
-    int64_t base;
-    if (contig) {
-      const int64_t row = grp * P + p;
-      ok = row < g.rows;
-      base = row * g.pitch;
-    } else {
-      // 32-bit divisions (an element holds fewer than 2^31 samples)
-      const uint32_t inner = static_cast<uint32_t>(axis_stride);
-      const uint32_t gpo = (inner + P - 1) / P;
-      const uint32_t o = static_cast<uint32_t>(grp) / gpo;
-      const uint32_t c = (static_cast<uint32_t>(grp) - o * gpo) * P + p;
-      ok = c < inner && (c % static_cast<uint32_t>(g.pitch)) < static_cast<uint32_t>(n_last);
-      base = static_cast<int64_t>(o) * n * inner + c;
-    }
-    base_s[p] = base;
-    ok_s[p] = ok ? 1 : 0;
-  }
-  const int64_t step = contig ? 1 : axis_stride;
-  __syncthreads();
-  int32_t valid = 0;
-  if (a.bytes && threadIdx.x == 0) {
-    for (int p = 0; p < P; ++p) valid += ok_s[p];
-  }
-  unsigned long long acct = 0;
-  const int64_t eoff = b * g.field;
-  const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
-  const bool box = a.op == static_cast<int>(CubeOp::kBox);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // this thread's line and first sample in the staging and the store
-  const int my_p = contig ? warp / Roles::kWpl : (threadIdx.x & (P - 1));
-  const int32_t my_i0 = contig ? lane + 32 * (warp % Roles::kWpl) : static_cast<int32_t>(threadIdx.x / P);
-  const int32_t my_di = contig ? Roles::kRowStride : Roles::kColStride;
-  const int my_dp = contig ? kWarps / Roles::kWpl : P;  // line stride of this thread (rows: P > kWarps)
-  const int32_t nw = contig ? static_cast<int32_t>(g.pitch) : n;  // samples written per line
+  const int32_t LS = ROWS ? row_stride<T>(n) : 1;  // line stride in shared memory
+  const int32_t gel = group_elems<T>(n, P, ROWS);
+  T* V0 = reinterpret_cast<T*>(smem_raw);
+  T* V1 = V0 + gel;
+  T* R = V1 + gel;
+  T* tot = R + gel;
   const int32_t j_begin = a.rung_loop ? 0 : static_cast<int32_t>(blockIdx.z);
-  const int32_t j_end = a.rung_loop ? a.rungs : j_begin + 1;
-  bool staged = false;  // V holds the staged shared input (first pass with a rung loop)
-  for (int32_t j = j_begin; j < j_end; ++j) {
-    const int32_t w = a.win[static_cast<int64_t>(j) * g.batch + b];
-    if (w < 1) continue;
-    const Win q = make_win(n, w);
-    double fac = 1.0;
-    if (box && a.last) {
-      double prod = 1.0;
+  const int32_t nr = a.rung_loop ? a.rungs : 1;
+  const bool box = a.op == static_cast<int>(CubeOp::kBox);
+  const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
+  // the windows of this CTA's rungs, once
+  if (threadIdx.x == 0) any_s = 0;
+  __syncthreads();
+  for (int32_t jj = threadIdx.x; jj < nr; jj += kThreads) {
+    const int32_t w = a.win[static_cast<int64_t>(j_begin + jj) * g.batch + b];
+    Win q{};
+    if (w >= 1) {
+      q = make_win(n, w);
+      any_s = 1;
+      if (box && a.last) {
+        double prod = 1.0;
 #pragma unroll
-      for (int ax = 0; ax < kMaxDim; ++ax) {
-        if (ax < g.dim) prod *= static_cast<double>(2 * min((w - 1) / 2, g.n[ax] - 1) + 1);
+        for (int ax = 0; ax < kMaxDim; ++ax) {
+          if (ax < g.dim) prod *= static_cast<double>(2 * min((w - 1) / 2, g.n[ax] - 1) + 1);
+        }
+        fac_s[jj] = static_cast<T>(1.0 / prod);
       }
-      fac = static_cast<double>(static_cast<T>(1.0 / prod));
     }
-    for (int f = 0; f < nf; ++f) {
-      // stage field f (the input of this rung) as values (box) or order keys (max / min)
-      const bool shared_in = a.in_stride == 0 && (f == 0 || a.in1 == nullptr);
-      if (!(staged && shared_in)) {
-        const T* src = (f == 0 || a.in1 == nullptr) ? a.in0 : a.in1;
-        if (src) src += static_cast<int64_t>(j) * a.in_stride + eoff;
-        const uint8_t* bits = a.bits ? a.bits + eoff : nullptr;
-        for (int p = my_p; p < P; p += my_dp) {
-          if (!ok_s[p]) continue;
-          const int64_t base = base_s[p];
-          // kStageLoads independent loads in flight per thread before their shared-memory stores
-          for (int32_t i0 = my_i0; i0 < n; i0 += kStageLoads * my_di) {
-            T v[kStageLoads];
-#pragma unroll
-            for (int u = 0; u < kStageLoads; ++u) {
-              const int32_t i = i0 + u * my_di;
-              if (i < n) {
-                const int64_t at = base + static_cast<int64_t>(i) * step;
-                v[u] = bits ? (((bits[at] >> a.bit) & 1u) ? T(1) : T(0)) : src[at];
-              }
-            }
-#pragma unroll
-            for (int u = 0; u < kStageLoads; ++u) {
-              const int32_t i = i0 + u * my_di;
-              if (i < n) V[i * PP + p] = box ? v[u] : okey(v[u]);
-            }
-          }
-        }
-        __syncthreads();
-        staged = shared_in;
-        acct += static_cast<unsigned long long>(valid) * n * (bits ? 1u : sizeof(T));
+    win_s[jj] = q;  // wa == 0: the rung skips this element
+  }
+  __syncthreads();
+  if (!any_s) return;
+  const int64_t g0 = static_cast<int64_t>(blockIdx.x) * a.gpc;
+  const int64_t ng = min(static_cast<int64_t>(a.gpc), a.groups - g0);
+  if (ng <= 0) return;
+  const int64_t eoff = b * g.field;
+  // one staging per group when every rung and field reads the same input, else one per field
+  const bool shared_in = a.in_stride == 0 && (nf == 1 || a.in1 == nullptr);
+  const int nst = shared_in ? 1 : nf;
+  const int64_t S = ng * nst;
+  const bool async = a.vec && a.bits == nullptr && (ROWS || P >= VW);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // copy roles. Rows: kWpl warps per line, lanes over 16-byte units. Column panels: QP units per
+  // panel row, threads over rows.
+  constexpr int kWpl = P >= kWarps ? 1 : kWarps / P;
+  constexpr int QP = P >= VW ? P / VW : 1;
+  const int r_p = warp / kWpl;
+  const int32_t r_u0 = lane + 32 * (warp % kWpl);
+  const int32_t r_du = 32 * kWpl;
+  const int c_q = threadIdx.x % QP;
+  const int32_t c_i0 = threadIdx.x / QP;
+  const int32_t c_di = kThreads / QP;
+  const auto src_of = [&](int f) -> const T* {
+    const T* s = (f == 0 || a.in1 == nullptr) ? a.in0 : a.in1;
+    return s + static_cast<int64_t>(j_begin) * a.in_stride + eoff;
+  };
+  // issue the 16-byte copies of one staging (async mode)
+  const auto issue = [&](T* Vb, const GroupPos& s, const T* src) {
+    if constexpr (ROWS) {
+      if ((s.mask >> r_p) & 1u) {
+        const int32_t units = (n + VW - 1) / VW;
+        const T* line = src + s.base + static_cast<int64_t>(r_p) * g.pitch;
+        T* dst = Vb + r_p * LS;
+        for (int32_t u = r_u0; u < units; u += r_du) cp_async16(dst + u * VW, line + u * VW);
       }
-      const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-      if (box) run_stage<T, kOpSum, P>(V, R, tot, n, TS, q);
-      else if (is_min) run_stage<T, kOpMinK, P>(V, R, tot, n, TS, q);
-      else run_stage<T, kOpMaxK, P>(V, R, tot, n, TS, q);
-      // store (pads of the contiguous axis written as 0)
-      T* dst = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + eoff;
-      acct += static_cast<unsigned long long>(valid) * n * sizeof(T);
-      const bool detsq = box && a.last && a.epi == static_cast<int>(BoxEpi::kDetSq);
-      const T* aux = detsq ? a.aux + eoff : nullptr;
-      for (int p = my_p; p < P; p += my_dp) {
-        if (!ok_s[p]) continue;
-        const int64_t base = base_s[p];
-        for (int32_t i = my_i0; i < nw; i += my_di) {
-          const int64_t at = base + static_cast<int64_t>(i) * step;
-          if (i >= n) {
-            dst[at] = T(0);
-            continue;
-          }
-          T y = R[i * PP + p];
-          if (!box) {
-            y = okey(y);
-          } else if (a.last) {
-            y = mul_rn(y, static_cast<T>(fac));
-            if (detsq) {
-              const T d = sub_rn(aux[at], y);
-              y = mul_rn(d, d);
-            }
-          }
-          dst[at] = y;
+    } else {
+      if (s.mask) {
+        const T* col = src + s.base + c_q * VW;
+        for (int32_t i = c_i0; i < n; i += c_di) cp_async16(Vb + i * P + c_q * VW, col + static_cast<int64_t>(i) * step);
+      }
+    }
+  };
+  // order keys in place over the units this thread copied (async mode, max / min)
+  const auto keys = [&](T* Vb, const GroupPos& s) {
+    if constexpr (ROWS) {
+      if ((s.mask >> r_p) & 1u) {
+        const int32_t units = (n + VW - 1) / VW;
+        T* line = Vb + r_p * LS;
+        for (int32_t u = r_u0; u < units; u += r_du) {
+          T* v = line + u * VW;
+#pragma unroll
+          for (int k = 0; k < VW; ++k) v[k] = okey(v[k]);
         }
       }
-      __syncthreads();  // the next stage rewrites R and tot
+    } else {
+      if (s.mask) {
+        for (int32_t i = c_i0; i < n; i += c_di) {
+          T* v = Vb + i * P + c_q * VW;
+#pragma unroll
+          for (int k = 0; k < VW; ++k) v[k] = okey(v[k]);
+        }
+      }
+    }
+  };
+  // synchronous staging (bit-field input, unaligned pointers, narrow column panels)
+  const auto stage_sync = [&](T* Vb, const GroupPos& s, int f) {
+    const T* src = a.bits ? nullptr : src_of(f);
+    const uint8_t* bits = a.bits ? a.bits + eoff : nullptr;
+    if constexpr (ROWS) {
+      if ((s.mask >> r_p) & 1u) {
+        const int64_t line = s.base + static_cast<int64_t>(r_p) * g.pitch;
+        for (int32_t i = r_u0; i < n; i += r_du) {
+          const T v = bits ? (((bits[line + i] >> a.bit) & 1u) ? T(1) : T(0)) : src[line + i];
+          Vb[r_p * LS + i] = box ? v : okey(v);
+        }
+      }
+    } else {
+      if (s.mask) {
+        const int p = threadIdx.x % P;
+        for (int32_t i = threadIdx.x / P; i < n; i += kThreads / P) {
+          const int64_t at = s.base + static_cast<int64_t>(i) * step + p;
+          const T v = bits ? (((bits[at] >> a.bit) & 1u) ? T(1) : T(0)) : src[at];
+          Vb[i * P + p] = box ? v : okey(v);
+        }
+      }
+    }
+  };
+  const bool detsq = box && a.last && a.epi == static_cast<int>(BoxEpi::kDetSq);
+  const auto epi = [&](T y, T fac, T auxv) -> T {
+    if (!box) return okey(y);
+    if (a.last) {
+      y = mul_rn(y, fac);
+      if (detsq) {
+        const T d = sub_rn(auxv, y);
+        y = mul_rn(d, d);
+      }
+    }
+    return y;
+  };
+  // the store of R as field f of rung j (pads of the contiguous axis written as 0)
+  const auto store = [&](const GroupPos& s, int32_t j, int f, T fac) {
+    T* dst = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + eoff;
+    const T* aux = detsq ? a.aux + eoff : nullptr;
+    if constexpr (ROWS) {
+      if (!((s.mask >> r_p) & 1u)) return;
+      const int64_t line = s.base + static_cast<int64_t>(r_p) * g.pitch;
+      const T* rl = R + r_p * LS;
+      if (a.vec) {
+        const int32_t units = static_cast<int32_t>(g.pitch) / VW;
+        for (int32_t u = r_u0; u < units; u += r_du) {
+          const int32_t i0 = u * VW;
+          V16 yv = *reinterpret_cast<const V16*>(rl + i0);
+          V16 av{};
+          if (detsq) av = *reinterpret_cast<const V16*>(aux + line + i0);
+          T* y = reinterpret_cast<T*>(&yv);
+          const T* ax = reinterpret_cast<const T*>(&av);
+#pragma unroll
+          for (int k = 0; k < VW; ++k) y[k] = i0 + k < n ? epi(y[k], fac, ax[k]) : T(0);
+          *reinterpret_cast<V16*>(dst + line + i0) = yv;
+        }
+      } else {
+        for (int32_t i = r_u0; i < static_cast<int32_t>(g.pitch); i += r_du) {
+          dst[line + i] = i < n ? epi(rl[i], fac, detsq ? aux[line + i] : T(0)) : T(0);
+        }
+      }
+    } else {
+      if (!s.mask) return;
+      if (a.vec && P >= VW) {
+        uint32_t live = 0;  // this thread's columns left of the row padding
+#pragma unroll
+        for (int k = 0; k < VW; ++k) live |= ((s.mask >> (c_q * VW + k)) & 1u) << k;
+        for (int32_t i = c_i0; i < n; i += c_di) {
+          const int64_t at = s.base + static_cast<int64_t>(i) * step + c_q * VW;
+          V16 yv = *reinterpret_cast<const V16*>(R + i * P + c_q * VW);
+          V16 av{};
+          if (detsq) av = *reinterpret_cast<const V16*>(aux + at);
+          T* y = reinterpret_cast<T*>(&yv);
+          const T* ax = reinterpret_cast<const T*>(&av);
+#pragma unroll
+          for (int k = 0; k < VW; ++k) y[k] = ((live >> k) & 1u) ? epi(y[k], fac, ax[k]) : T(0);
+          *reinterpret_cast<V16*>(dst + at) = yv;
+        }
+      } else {
+        const int p = threadIdx.x % P;
+        if (!((s.mask >> p) & 1u)) return;
+        for (int32_t i = threadIdx.x / P; i < n; i += kThreads / P) {
+          const int64_t at = s.base + static_cast<int64_t>(i) * step + p;
+          dst[at] = epi(R[i * P + p], fac, detsq ? aux[at] : T(0));
+        }
+      }
+    }
+  };
+  unsigned long long acct = 0;
+  GroupPos cur = group_at<P, ROWS>(g, g0, n, inner);
+  group_finish<P, ROWS>(cur, g, n, inner);
+  GroupPos nxt = cur;  // the group of the staging in flight
+  if (async) {
+    issue(V0, cur, src_of(0));
+    cp_async_commit();
+  }
+  for (int64_t st = 0; st < S; ++st) {
+    T* Vb = (st & 1) ? V1 : V0;
+    const int f_st = nst == 1 ? 0 : static_cast<int>(st & 1);
+    if (async) {
+      if (st + 1 < S) {
+        const int f_next = nst == 1 ? 0 : static_cast<int>((st + 1) & 1);
+        if (f_next == 0) {
+          group_next<P, ROWS>(nxt, g, n, inner);
+          group_finish<P, ROWS>(nxt, g, n, inner);
+        }
+        issue((st & 1) ? V0 : V1, nxt, src_of(f_next));
+      }
+      cp_async_commit();
+      cp_async_wait_prior();
+      if (!box) keys(Vb, cur);
+    } else {
+      stage_sync(Vb, cur, f_st);
+    }
+    __syncthreads();
+    const int32_t valid = __popc(cur.mask);
+    if (a.bytes && threadIdx.x == 0) acct += static_cast<unsigned long long>(valid) * n * (a.bits ? 1u : sizeof(T));
+    if (cur.mask) {
+      const int32_t jn = shared_in ? nr : 1;
+      for (int32_t jj = 0; jj < jn; ++jj) {
+        const Win q = win_s[jj];
+        if (q.wa == 0) continue;
+        const T fac = box && a.last ? fac_s[jj] : T(1);
+        const int f_lo = shared_in ? 0 : f_st;
+        const int f_hi = shared_in ? nf : f_st + 1;
+        for (int f = f_lo; f < f_hi; ++f) {
+          const bool is_min =
+              a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
+          if (box) run_stage<T, kOpSum, P, PP>(Vb, R, tot, n, TS, q, LS);
+          else if (is_min) run_stage<T, kOpMinK, P, PP>(Vb, R, tot, n, TS, q, LS);
+          else run_stage<T, kOpMaxK, P, PP>(Vb, R, tot, n, TS, q, LS);
+          store(cur, j_begin + jj, f, fac);
+          if (a.bytes && threadIdx.x == 0) acct += static_cast<unsigned long long>(valid) * n * sizeof(T);
+          __syncthreads();  // the next stage rewrites R and tot
+        }
+      }
+    }
+    // the next staging: a new group after the last field of this one
+    if (nst == 1 || (st & 1)) {
+      group_next<P, ROWS>(cur, g, n, inner);
+      group_finish<P, ROWS>(cur, g, n, inner);
     }
   }
   if (a.bytes && threadIdx.x == 0 && acct) atomicAdd(a.bytes, acct);
 }
 
-size_t smem_bytes(int32_t n, int P, size_t es) {
-  return (static_cast<size_t>(2) * n + static_cast<size_t>(2) * tot_slots(n)) * static_cast<size_t>(line_pitch(P)) * es;
+size_t smem_bytes(int32_t n, int P, bool rows, size_t es) {
+  const int32_t gel = es == 4 ? group_elems<float>(n, P, rows) : group_elems<double>(n, P, rows);
+  return (static_cast<size_t>(3) * gel + static_cast<size_t>(2) * tot_slots(n) * P) * es;
 }
 
 template <class T>
 void allow_smem(int bytes) {
-  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  EDAB_CUDA(cudaFuncSetAttribute(cube_pass<T, 8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
 struct DevFacts {
   int sms = 148;
-  size_t smem = 227 * 1024;
+  size_t smem = 227 * 1024;  // dynamic shared memory a CTA may take
+  size_t sm_smem = 228 * 1024;  // shared memory of an SM
 };
 DevFacts dev_facts() {
   static std::mutex mu;
@@ -598,11 +800,13 @@ DevFacts dev_facts() {
   EDAB_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
   if (!have[dev]) {
-    int optin = 0, sms = 0;
+    int optin = 0, sms = 0, per_sm = 0;
     EDAB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     EDAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    EDAB_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     f[dev].sms = sms;
-    f[dev].smem = static_cast<size_t>(optin) - 1024;  // the kernel's static shared memory
+    f[dev].smem = static_cast<size_t>(optin) - 2048;  // the kernel's static shared memory
+    f[dev].sm_smem = static_cast<size_t>(per_sm);
     allow_smem<float>(static_cast<int>(f[dev].smem));
     allow_smem<double>(static_cast<int>(f[dev].smem));
     have[dev] = true;
@@ -610,50 +814,78 @@ DevFacts dev_facts() {
   return f[dev];
 }
 
-// Lines per CTA (a power of two up to 32): 8 lines for column panels (whole sectors, and shared
-// memory for several CTAs per SM), rows up to 8 per CTA; fewer where the shared memory or the
-// element's rows run out.
+// Lines per group (a power of two up to 8): 8 lines for column panels (whole sectors) and rows;
+// fewer where the element's rows run out or the shared memory would hold fewer than two CTAs.
 template <class T>
 int lines_per_cta(const Geom& g, int axis, size_t cap) {
   const int32_t n = g.n[axis];
+  const bool rows = axis == g.dim - 1;
   int P = 8;
-  if (axis == g.dim - 1) {
+  if (rows) {
     while (P > 1 && P / 2 >= g.rows) P /= 2;
-  } else {
-    while (P > 1 && P / 2 >= g.stride[axis]) P /= 2;
   }
-  while (P > 1 && smem_bytes(n, P, sizeof(T)) > cap / 2) P /= 2;
-  if (smem_bytes(n, P, sizeof(T)) > cap) {
+  while (P > 1 && smem_bytes(n, P, rows, sizeof(T)) > cap / 2) P /= 2;
+  if (smem_bytes(n, P, rows, sizeof(T)) > cap) {
     throw std::invalid_argument("edab: an axis of " + std::to_string(n) + " samples exceeds the shared-memory line capacity");
   }
   return P;
 }
 
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 template <class T>
 void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   const DevFacts f = dev_facts();
+  const bool rows = a.axis == g.dim - 1;
   const int P = lines_per_cta<T>(g, a.axis, f.smem);
+  if (a.rungs > kMaxRungs) throw std::invalid_argument("edab: more rungs than a cube launch holds");
   int64_t groups;
-  if (a.axis == g.dim - 1) {
+  if (rows) {
     groups = (g.rows + P - 1) / P;
   } else {
     int64_t outer = 1;
     for (int ax = 0; ax < a.axis; ++ax) outer *= g.n[ax];
-    groups = outer * ((g.stride[a.axis] + P - 1) / P);
+    groups = outer * (g.stride[a.axis] / P);
   }
-  if (groups > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: cube launch too large");
-  const dim3 grid(static_cast<unsigned>(groups), static_cast<unsigned>(g.batch), a.rung_loop ? 1u : static_cast<unsigned>(a.rungs));
-  const size_t smem = smem_bytes(g.n[a.axis], P, sizeof(T));
+  const size_t smem = smem_bytes(g.n[a.axis], P, rows, sizeof(T));
+  // line groups per CTA: the fewest waves of CTAs times the groups a CTA runs (plus one for its
+  // setup and the first copy), more groups per CTA on a tie
+  const int64_t slots = static_cast<int64_t>(f.sms) * std::max<int64_t>(1, static_cast<int64_t>(f.sm_smem / (smem + 3072)));
+  const int64_t resident = std::min<int64_t>(slots, static_cast<int64_t>(f.sms) * 4);
+  const int64_t zc = a.rung_loop ? 1 : a.rungs;
+  int gpc = 1;
+  double best = 0.0;
+  for (int c = 1; c <= kMaxGroupsPerCta; ++c) {
+    const int64_t ctas = (groups + c - 1) / c * g.batch * zc;
+    const double cost = static_cast<double>((ctas + resident - 1) / resident) * (c + 1);
+    if (c == 1 || cost <= best) {
+      best = cost;
+      gpc = c;
+    }
+  }
+  const int64_t gx = (groups + gpc - 1) / gpc;
+  if (gx > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: cube launch too large");
+  a.groups = groups;
+  a.gpc = gpc;
+  const int64_t es = static_cast<int64_t>(sizeof(T));
+  a.vec = aligned16(a.in0) && aligned16(a.in1) && aligned16(a.out0) && aligned16(a.out1) && aligned16(a.aux) &&
+          (a.in_stride * es) % 16 == 0 && (a.out_stride * es) % 16 == 0 && (g.field * es) % 16 == 0 &&
+          (g.pitch * es) % 16 == 0 && (rows || (g.stride[a.axis] * es) % 16 == 0);
+  const dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(g.batch), a.rung_loop ? 1u : static_cast<unsigned>(a.rungs));
   a.bytes = cube_bytes_counter();
   profile_cube_launch(s, true);
+#define EDAB_CUBE_LAUNCH(PV)                                                    \
+  do {                                                                          \
+    if (rows) cube_pass<T, PV, true><<<grid, kThreads, smem, s>>>(g, a);        \
+    else cube_pass<T, PV, false><<<grid, kThreads, smem, s>>>(g, a);            \
+  } while (0)
   switch (P) {
-    case 1: cube_pass<T, 1><<<grid, kThreads, smem, s>>>(g, a); break;
-    case 2: cube_pass<T, 2><<<grid, kThreads, smem, s>>>(g, a); break;
-    case 4: cube_pass<T, 4><<<grid, kThreads, smem, s>>>(g, a); break;
-    case 8: cube_pass<T, 8><<<grid, kThreads, smem, s>>>(g, a); break;
-    case 16: cube_pass<T, 16><<<grid, kThreads, smem, s>>>(g, a); break;
-    default: cube_pass<T, 32><<<grid, kThreads, smem, s>>>(g, a); break;
+    case 1: EDAB_CUBE_LAUNCH(1); break;
+    case 2: EDAB_CUBE_LAUNCH(2); break;
+    case 4: EDAB_CUBE_LAUNCH(4); break;
+    default: EDAB_CUBE_LAUNCH(8); break;
   }
+#undef EDAB_CUBE_LAUNCH
   EDAB_LAUNCH("cube_pass");
   profile_cube_launch(s, false);
 }

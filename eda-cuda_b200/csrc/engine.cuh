@@ -74,6 +74,8 @@ struct Geom {
   int32_t n_max;
   int32_t n_last;            // n[dim - 1] (device code reads this, not n[] at a run-time index)
   uint64_t pitch_inv;        // ceil(2^64 / pitch): v / pitch = umulhi(v, pitch_inv) for 0 <= v < 2^32
+  uint64_t field_inv;        // ceil(2^64 / field): i / field = umulhi(i, field_inv) for 0 <= i < 2^64 / field
+  int32_t field_fast;        // batch field^2 <= 2^64: every sample index of the batch divides by umulhi
 };
 Geom make_geom(int dim, int64_t batch, const int64_t* n);
 
@@ -94,9 +96,21 @@ __host__ __device__ inline int64_t pitch_row(const Geom& g, int64_t v) {
 }
 __host__ __device__ inline int64_t pitch_col(const Geom& g, int64_t v) { return v - pitch_row(g, v) * g.pitch; }
 __host__ __device__ inline bool is_pad(const Geom& g, int64_t v) { return pitch_col(g, v) >= g.n_last; }
+// Element of sample index i of the batch (i / field without a 64-bit division where exact).
+__host__ __device__ inline int64_t elem_of(const Geom& g, int64_t i) {
+#ifdef __CUDA_ARCH__
+  if (g.field_fast) return static_cast<int64_t>(__umul64hi(static_cast<uint64_t>(i), g.field_inv));
+#endif
+  return i / g.field;
+}
+// Coordinate along axis a of padded offset v (v < field < 2^31: the row index fits 32 bits).
 __host__ __device__ inline int32_t coord_of(const Geom& g, int64_t v, int a) {
-  if (a == g.dim - 1) return static_cast<int32_t>(pitch_col(g, v));
-  return static_cast<int32_t>((v / geom_stride(g, a)) % geom_n(g, a));
+  const int64_t row = pitch_row(g, v);
+  if (a == g.dim - 1) return static_cast<int32_t>(v - row * g.pitch);
+  const uint32_t r32 = static_cast<uint32_t>(row);
+  if (g.dim == 2) return static_cast<int32_t>(r32);  // a == 0: rows are the axis-0 index
+  const uint32_t n1 = static_cast<uint32_t>(g.n[1]);  // dim 3: row = x0 n1 + x1
+  return static_cast<int32_t>(a == 1 ? r32 % n1 : r32 / n1);
 }
 // Coordinates of padded offset v; false for a pad.
 __host__ __device__ inline bool voxel_coords(const Geom& g, int64_t v, int32_t* x) {
@@ -104,11 +118,12 @@ __host__ __device__ inline bool voxel_coords(const Geom& g, int64_t v, int32_t* 
   const int64_t col = v - row * g.pitch;
   if (col >= g.n_last) return false;
   x[g.dim - 1] = static_cast<int32_t>(col);
-  int64_t q = row;
-  for (int a = g.dim - 2; a >= 0; --a) {
-    x[a] = static_cast<int32_t>(q % g.n[a]);
-    q /= g.n[a];
+  uint32_t q = static_cast<uint32_t>(row);  // row < field < 2^31
+  for (int a = g.dim - 2; a >= 1; --a) {
+    x[a] = static_cast<int32_t>(q % static_cast<uint32_t>(g.n[a]));
+    q /= static_cast<uint32_t>(g.n[a]);
   }
+  if (g.dim >= 2) x[0] = static_cast<int32_t>(q);  // the outermost index needs no modulo
   return true;
 }
 
@@ -119,12 +134,13 @@ __device__ __forceinline__ bool voxel_coords_d(const Geom& g, int64_t v, int32_t
   const int64_t col = v - row * g.pitch;
   if (col >= g.n[D - 1]) return false;
   x[D - 1] = static_cast<int32_t>(col);
-  int64_t q = row;
+  uint32_t q = static_cast<uint32_t>(row);  // row < field < 2^31
 #pragma unroll
-  for (int a = D - 2; a >= 0; --a) {
-    x[a] = static_cast<int32_t>(q % g.n[a]);
-    q /= g.n[a];
+  for (int a = D - 2; a >= 1; --a) {
+    x[a] = static_cast<int32_t>(q % static_cast<uint32_t>(g.n[a]));
+    q /= static_cast<uint32_t>(g.n[a]);
   }
+  if constexpr (D >= 2) x[0] = static_cast<int32_t>(q);  // the outermost index needs no modulo
   return true;
 }
 

@@ -55,6 +55,10 @@ Geom make_geom(int dim, int64_t batch, const int64_t* n) {
   g.rows = g.field / g.pitch;
   g.n_last = g.n[dim - 1];
   g.pitch_inv = ~uint64_t{0} / static_cast<uint64_t>(g.pitch) + 1;
+  g.field_inv = ~uint64_t{0} / static_cast<uint64_t>(g.field) + 1;
+  // i < batch field <= 2^64 / field keeps umulhi(i, field_inv) exact
+  const long double f = static_cast<long double>(g.field);
+  g.field_fast = static_cast<long double>(batch) * f * f <= 18446744073709551616.0L ? 1 : 0;
   return g;
 }
 
@@ -727,7 +731,7 @@ void Engine<T>::scale_field() {
   const T* om = om_;
   const auto runW = [=] __device__(int64_t b) { return on[b] && wW[b] >= 1; };
   for_samples(s_, B_ * g_.field, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     if (on[b] && wW[b] >= 1) marks[i] = 0;
   });
   for_voxels(s_, g_, runW, [=] __device__(int64_t b, int64_t, int64_t i) {
@@ -956,7 +960,7 @@ void Engine<T>::g2() {
   uint8_t* Pacc = Pacc_;
   const Geom g = g_;
   for_samples(s_, B_ * g_.field, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     if (onfine[b]) Pacc[i] = el[b].g2_slot ? P1[i] : P0[i];
   });
   // G3: the coarse median of the raw window outside the population's reach
@@ -978,7 +982,7 @@ void Engine<T>::g2() {
   cube_simple<T>(s_, g_, CubeOp::kMax, t1, t1, nullptr, w3r);
   uint8_t* sel = selm_;
   for_samples(s_, B_ * g_.field, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     if (!onfine[b]) return;
     sel[i] = (!is_pad(g, i - b * g.field) && t1[i] < T(0.5) && omc[i] < inf_t<T>()) ? 1 : 0;
   });
@@ -1376,7 +1380,7 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
   // start (cpp/src/method/driver.cpp:393-420): the padded copy, the prescale by 2^-ilogb(max|x|)
   const int32_t nl = g_.n_last;
   for_samples(s_, B_ * g_.field, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     const int64_t v = i - b * g.field;
     const int64_t q = pitch_row(g, v);
     const int64_t t = v - q * g.pitch;

@@ -197,7 +197,11 @@ __device__ __forceinline__ bool sel_item(const Geom& g, const SelView<T>& a, int
     if (a.sel.mask != nullptr && (a.sel.mask[i] & a.sel.bits) == 0) return false;
     val = static_cast<double>(a.sel.field[i]);
   } else {
+#ifdef __CUDA_ARCH__
+    const int64_t k = static_cast<int64_t>(__umul64hi(static_cast<uint64_t>(t), g.field_inv));  // t < 3 field
+#else
     const int64_t k = t / g.field;
+#endif
     const int64_t v = t - k * g.field;
     const int axis = k == 0 ? a.ax[0] : (k == 1 ? a.ax[1] : a.ax[2]);
     if (is_pad(g, v) || coord_of(g, v, axis) >= geom_n(g, axis) - 1) return false;
@@ -537,18 +541,22 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   const int64_t step = contig ? 1 : geom_stride(g, axis);
   const int64_t eoff = b * g.field;
   __syncthreads();
-  const int32_t total = P * n;
-  for (int32_t t = threadIdx.x; t < total; t += blockDim.x) {
-    int p, i;
-    if (contig) {
-      p = t / n;
-      i = t - p * n;
-    } else {
-      i = t / P;
-      p = t - i * P;
+  if (contig) {
+    // lines in turn, consecutive samples over the threads
+    for (int p = 0; p < P; ++p) {
+      if (!ok_s[p]) continue;
+      const T* src = r + eoff + base_s[p];
+      for (int32_t i = threadIdx.x; i < n; i += blockDim.x) X[p * n + i] = src[i];
     }
-    if (!ok_s[p]) continue;
-    X[p * n + i] = r[eoff + base_s[p] + i * step];
+  } else {
+    // the P columns of a row over consecutive threads (whole sectors); one division per thread
+    const int32_t rows_per = static_cast<int32_t>(blockDim.x) / P;
+    const int p = static_cast<int>(threadIdx.x % P);
+    const int32_t i0 = static_cast<int32_t>(threadIdx.x / P);
+    if (i0 < rows_per && ok_s[p]) {
+      const T* src = r + eoff + base_s[p];
+      for (int32_t i = i0; i < n; i += rows_per) X[p * n + i] = src[static_cast<int64_t>(i) * step];
+    }
   }
   __syncthreads();
   for (int32_t t = threadIdx.x; t < P * nb; t += blockDim.x) {
@@ -568,10 +576,9 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   }
   __syncthreads();
   int mine = 0;
-  for (int32_t t = threadIdx.x; t < total; t += blockDim.x) {
-    const int p = t / n;
-    const int32_t s = t - p * n;
-    if (!ok_s[p] || s < 1 || s > n - 2) continue;
+  for (int p = 0; p < P; ++p) {
+   if (!ok_s[p]) continue;
+   for (int32_t s = 1 + threadIdx.x; s <= n - 2; s += blockDim.x) {
     const T* x = X + p * n;
     const T cur = x[s], prev = x[s - 1];
     if (!(prev < cur || prev > cur)) continue;
@@ -610,6 +617,7 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
       flags[at] |= static_cast<uint8_t>(1u << axis);
       ++mine;
     }
+   }
   }
   for (int d = 16; d > 0; d >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, d);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&count_s, mine);
@@ -654,7 +662,7 @@ __device__ __forceinline__ void unite(int32_t* L, int32_t a, int32_t c) {
 template <class T>
 void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t* flags, Elem* el, const int32_t* run) {
   for_samples(s, g.batch * g.field, [=] __device__(int64_t i) {
-    if (run == nullptr || run[i / g.field]) flags[i] = 0;
+    if (run == nullptr || run[elem_of(g, i)]) flags[i] = 0;
   });
   int optin = 0, dev = 0;
   EDAB_CUDA(cudaGetDevice(&dev));
@@ -692,13 +700,13 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
 void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32_t* labels, const int32_t* run) {
   const int64_t total = g.batch * g.field;
   for_samples(s, total, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     if (run && !run[b]) return;
     const int64_t v = i - b * g.field;
     labels[i] = (!is_pad(g, v) && (mask[i] & bits) != 0) ? static_cast<int32_t>(v) : -1;
   });
   for_samples(s, total, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     if (run && !run[b]) return;
     int32_t* L = labels + b * g.field;
     const int32_t v = static_cast<int32_t>(i - b * g.field);
@@ -711,7 +719,7 @@ void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32
     }
   });
   for_samples(s, total, [=] __device__(int64_t i) {
-    const int64_t b = i / g.field;
+    const int64_t b = elem_of(g, i);
     if (run && !run[b]) return;
     int32_t* L = labels + b * g.field;
     const int32_t v = static_cast<int32_t>(i - b * g.field);

@@ -23,7 +23,7 @@ __global__ void to_padded(Geom g, const T* __restrict__ x, T* __restrict__ f) {
   const int64_t total = g.batch * g.field;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t b = i / g.field, v = i - b * g.field;
+    const int64_t b = elem_of(g, i), v = i - b * g.field;
     const int64_t col = v % g.pitch, row = v / g.pitch;
     const int32_t nl = g.n_last;
     f[i] = col < nl ? x[b * g.count + row * nl + col] : T(0);

@@ -125,6 +125,16 @@ def test_cube_on_benchmark_sized_images(dev):
     check(dev, (512, 512), "box", [7, 257], np.float32)
 
 
+def test_cube_on_a_full_benchmark_batch(dev):
+    """64 images of 512 x 512 with a different window per image (one skipped): every CTA runs
+    several line groups, copying the next group while it folds the current one; and a 3-rung
+    launch of the same batch (the first pass stages each group once for every rung)."""
+    wins = np.array([9, 33, 65, 0, 257, 1, 129, 17] * 8, np.int32)
+    check(dev, (512, 512), "maxmin", wins, np.float32)
+    check(dev, (512, 512), "box", wins, np.float32)
+    check(dev, (512, 512), "maxmin", np.stack([wins, np.roll(wins, 3), np.roll(wins, 5)]), np.float32, seed=77)
+
+
 def test_cube_on_the_longest_lines(dev):
     check(dev, (8192,), "box", [4095, 16383, 1], np.float32)
     check(dev, (4096,), "maxmin", [2047, 9], np.float64)
