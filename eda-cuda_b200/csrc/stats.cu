@@ -475,12 +475,19 @@ __device__ __forceinline__ int side_step(T u, T v, T tau) {
   return (Max ? deep<T>(v, u, tau) : deep<T>(u, v, tau)) ? 1 : 0;
 }
 
+// Sample k of a staged line: one pad word after every 32 samples (the lanes of a warp scanning
+// consecutive blocks hit distinct banks).
+template <class T>
+__device__ __forceinline__ T xs(const T* x, int32_t k) {
+  return x[k + (k >> 5)];
+}
+
 template <bool Max, int Dir, class T>
 __device__ bool side_deep(const T* x, int32_t n, int32_t p, T v, T tau, const T* bmin, const T* bmax) {
   const int32_t cp = p / kBlk;
   const int32_t lim = Dir < 0 ? cp * kBlk : min(cp * kBlk + kBlk - 1, n - 1);
   for (int32_t k = p + Dir; Dir < 0 ? k >= lim : k <= lim; k += Dir) {
-    const int st = side_step<Max>(x[k], v, tau);
+    const int st = side_step<Max>(xs(x, k), v, tau);
     if (st) return st == 1;
   }
   const int32_t nb = (n + kBlk - 1) / kBlk;
@@ -490,7 +497,7 @@ __device__ bool side_deep(const T* x, int32_t n, int32_t p, T v, T tau, const T*
       const int32_t k0 = Dir < 0 ? c * kBlk + kBlk - 1 : c * kBlk;
       const int32_t k1 = Dir < 0 ? c * kBlk : min(c * kBlk + kBlk - 1, n - 1);
       for (int32_t k = k0; Dir < 0 ? k >= k1 : k <= k1; k += Dir) {
-        const int st = side_step<Max>(x[k], v, tau);
+        const int st = side_step<Max>(xs(x, k), v, tau);
         if (st) return st == 1;
       }
       return false;
@@ -501,18 +508,21 @@ __device__ bool side_deep(const T* x, int32_t n, int32_t p, T v, T tau, const T*
   return false;
 }
 
+// Staged lines: P lines of LX words (sample k at k + k / 32; LX odd, so lanes on consecutive lines
+// hit distinct banks), then the block minima and maxima. Rows: threads over the samples of a line;
+// column panels: lanes over the panel's columns (coalesced tau reads and flag writes).
 template <class T>
 __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T* __restrict__ r,
                                                        const T* __restrict__ tau, uint8_t* __restrict__ flags,
-                                                       Elem* el, const int32_t* run, int P) {
+                                                       Elem* el, const int32_t* run, int P, int32_t LX) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
   const int32_t n = geom_n(g, axis);
   const bool contig = axis == g.dim - 1;
   const int32_t nb = (n + kBlk - 1) / kBlk;
-  T* X = reinterpret_cast<T*>(smem_raw);      // P x n
-  T* bmin = X + static_cast<int64_t>(P) * n;  // P x nb
+  T* X = reinterpret_cast<T*>(smem_raw);
+  T* bmin = X + static_cast<int64_t>(P) * LX;
   T* bmax = bmin + static_cast<int64_t>(P) * nb;
   __shared__ int64_t base_s[64];
   __shared__ int32_t ok_s[64];
@@ -546,7 +556,8 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
     for (int p = 0; p < P; ++p) {
       if (!ok_s[p]) continue;
       const T* src = r + eoff + base_s[p];
-      for (int32_t i = threadIdx.x; i < n; i += blockDim.x) X[p * n + i] = src[i];
+      T* x = X + p * LX;
+      for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[i + (i >> 5)] = src[i];
     }
   } else {
     // the P columns of a row over consecutive threads (whole sectors); one division per thread
@@ -555,7 +566,8 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
     const int32_t i0 = static_cast<int32_t>(threadIdx.x / P);
     if (i0 < rows_per && ok_s[p]) {
       const T* src = r + eoff + base_s[p];
-      for (int32_t i = i0; i < n; i += rows_per) X[p * n + i] = src[static_cast<int64_t>(i) * step];
+      T* x = X + p * LX;
+      for (int32_t i = i0; i < n; i += rows_per) x[i + (i >> 5)] = src[static_cast<int64_t>(i) * step];
     }
   }
   __syncthreads();
@@ -563,11 +575,11 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
     const int p = t / nb;
     const int32_t c = t - p * nb;
     if (!ok_s[p]) continue;
-    const T* x = X + p * n;
-    const int32_t i0 = c * kBlk, i1 = min(i0 + kBlk, n);
-    T mn = x[i0], mx = mn;
-    for (int32_t i = i0 + 1; i < i1; ++i) {
-      const T v = x[i];
+    const T* xb = X + p * LX + c * (kBlk + 1);  // block c, stored contiguously
+    const int32_t len = min(kBlk, n - c * kBlk);
+    T mn = xb[0], mx = mn;
+    for (int32_t i = 1; i < len; ++i) {
+      const T v = xb[i];
       mn = (v < mn || v != v) ? v : mn;
       mx = (v > mx || v != v) ? v : mx;
     }
@@ -576,20 +588,18 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   }
   __syncthreads();
   int mine = 0;
-  for (int p = 0; p < P; ++p) {
-   if (!ok_s[p]) continue;
-   for (int32_t s = 1 + threadIdx.x; s <= n - 2; s += blockDim.x) {
-    const T* x = X + p * n;
-    const T cur = x[s], prev = x[s - 1];
-    if (!(prev < cur || prev > cur)) continue;
-    // the run of samples equal to cur from s
+  // the run of samples equal to x[s] from s (s a run start): significant extremum -> flag its peak
+  const auto visit = [&](int p, int32_t s) {
+    const T* x = X + p * LX;
+    const T cur = xs(x, s), prev = xs(x, s - 1);
+    if (!(prev < cur || prev > cur)) return;
     const T* pmin = bmin + p * nb;
     const T* pmax = bmax + p * nb;
     int32_t e;
     {
       const int32_t lim = min((s / kBlk) * kBlk + kBlk - 1, n - 1);
       int32_t k = s + 1;
-      while (k <= lim && x[k] == cur) ++k;
+      while (k <= lim && xs(x, k) == cur) ++k;
       if (k <= lim || k >= n) {
         e = k - 1;
       } else {
@@ -597,17 +607,17 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
         for (int32_t c = k / kBlk; c < nb; ++c) {
           if (pmin[c] == cur && pmax[c] == cur) continue;
           k = c * kBlk;
-          while (x[k] == cur) ++k;
+          while (xs(x, k) == cur) ++k;
           e = k - 1;
           break;
         }
       }
     }
-    if (e > n - 2) continue;
-    const T nxt = x[e + 1];
+    if (e > n - 2) return;
+    const T nxt = xs(x, e + 1);
     const bool is_max = prev < cur && nxt < cur;
     const bool is_min = prev > cur && nxt > cur;
-    if (!is_max && !is_min) continue;
+    if (!is_max && !is_min) return;
     const int32_t pk = (s + e) / 2;
     const int64_t at = eoff + base_s[p] + pk * step;
     const T tp = tau[at];
@@ -617,7 +627,18 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
       flags[at] |= static_cast<uint8_t>(1u << axis);
       ++mine;
     }
-   }
+  };
+  if (contig) {
+    for (int p = 0; p < P; ++p) {
+      if (!ok_s[p]) continue;
+      for (int32_t s = 1 + threadIdx.x; s <= n - 2; s += blockDim.x) visit(p, s);
+    }
+  } else {
+    const int p = threadIdx.x & 31;
+    const int32_t nw = static_cast<int32_t>(blockDim.x >> 5);
+    if (p < P && ok_s[p]) {
+      for (int32_t s = 1 + static_cast<int32_t>(threadIdx.x >> 5); s <= n - 2; s += nw) visit(p, s);
+    }
   }
   for (int d = 16; d > 0; d >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, d);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&count_s, mine);
@@ -680,7 +701,8 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
     int P;
     if (a == g.dim - 1) P = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({static_cast<int64_t>(8192 / n), g.rows, 64})));
     else P = static_cast<int>(std::min<int64_t>(32, g.stride[a]));
-    const auto bytes = [&](int p) { return static_cast<size_t>(p) * (n + 2 * nb) * sizeof(T); };
+    const int32_t LX = (n + ((n - 1) >> 5) + 1) | 1;  // padded line words, odd
+    const auto bytes = [&](int p) { return static_cast<size_t>(p) * (LX + 2 * nb) * sizeof(T); };
     while (P > 1 && bytes(P) > cap) --P;
     if (bytes(P) > cap) throw std::invalid_argument("edab: a line exceeds the shared memory of the extrema pass");
     int64_t groups;
@@ -692,7 +714,7 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
       groups = outer * ((g.stride[a] + P - 1) / P);
     }
     flags_pass<T><<<dim3(static_cast<unsigned>(groups), static_cast<unsigned>(g.batch)), kThreads, bytes(P), s>>>(
-        g, a, r, tau, flags, el, run, P);
+        g, a, r, tau, flags, el, run, P, LX);
     EDAB_LAUNCH("flags_pass");
   }
 }
