@@ -121,9 +121,51 @@ void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) 
   cudaEventDestroy(done[1]);
 }
 
+// The rows of the runs come from a stream-ordered pool per device that keeps up to 2 GiB cached
+// between calls (no cudaMalloc / cudaFree, which synchronizes the device, per call); they are
+// returned on the pool's own stream once the run's work is complete (every call and collect ends
+// with a synchronization of its stream).
+RowsPool& rows_pool(int dev) {
+  static std::mutex mu;
+  static RowsPool pools[64];
+  std::lock_guard<std::mutex> lock(mu);
+  RowsPool& p = pools[dev];
+  if (!p.pool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    EDAB_CUDA(cudaMemPoolCreate(&p.pool, &props));
+    uint64_t keep = uint64_t{2} << 30;
+    EDAB_CUDA(cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    EDAB_CUDA(cudaStreamCreateWithFlags(&p.free_stream, cudaStreamNonBlocking));
+  }
+  return p;
+}
+
+void* rows_alloc(size_t bytes, cudaStream_t s, const char* what) {
+  int dev = 0;
+  EDAB_CUDA(cudaGetDevice(&dev));
+  void* p = nullptr;
+  const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, rows_pool(dev).pool, s);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    throw OutOfMemory(std::string("eda: ") + what + " (" + std::to_string(bytes >> 20) +
+                      " MiB) do not fit the device memory; set max_imf or decompose fewer elements per call");
+  }
+  EDAB_CUDA(e);
+  return p;
+}
+
 Run::~Run() {
-  if (dev_rows) cudaFree(dev_rows);
-  if (dev_orient) cudaFree(dev_orient);
+  if (!dev_rows && !dev_orient) return;
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess) return;
+  cudaSetDevice(device);
+  const cudaStream_t fs = rows_pool(device).free_stream;
+  if (dev_rows) cudaFreeAsync(dev_rows, fs);
+  if (dev_orient) cudaFreeAsync(dev_orient, fs);
+  cudaSetDevice(prev);
 }
 
 namespace {
@@ -321,23 +363,10 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
   run->rows_cap = cap;
   const size_t row_bytes = static_cast<size_t>(batch) * cap * static_cast<size_t>(g.count) * es;
   const size_t he = static_cast<size_t>(batch) * static_cast<size_t>(cap - 1);
-  {
-    const cudaError_t e = cudaMalloc(&run->dev_rows, row_bytes);
-    if (e == cudaErrorMemoryAllocation) {
-      (void)cudaGetLastError();
-      throw OutOfMemory("eda: the output rows (" + std::to_string(row_bytes >> 20) +
-                        " MiB) do not fit the device memory; set max_imf or decompose fewer elements per call");
-    }
-    EDAB_CUDA(e);
-  }
+  run->dev_rows = rows_alloc(row_bytes, s, "the output rows");
   if (p.orientation && dim >= 2) {
     const size_t ob = static_cast<size_t>(batch) * (cap - 1) * (dim + 1) * static_cast<size_t>(g.count) * es;
-    const cudaError_t e = cudaMalloc(&run->dev_orient, ob);
-    if (e == cudaErrorMemoryAllocation) {
-      (void)cudaGetLastError();
-      throw OutOfMemory("eda: the orientation rows (" + std::to_string(ob >> 20) + " MiB) do not fit the device memory");
-    }
-    EDAB_CUDA(e);
+    run->dev_orient = rows_alloc(ob, s, "the orientation rows");
     EDAB_CUDA(cudaMemsetAsync(run->dev_orient, 0, ob, s));
   }
   // the history: scale, sifts (int32), spacing, energy (double), [B, cap - 1] each

@@ -70,6 +70,15 @@ struct Params {
 };
 
 // One call's results: the rows (B, cap, count) on the device and the per-element information.
+// The stream-ordered pool of the runs' rows on one device and the stream they are returned on.
+struct RowsPool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t free_stream = nullptr;
+};
+RowsPool& rows_pool(int dev);
+// bytes from the current device's rows pool, ordered on stream s (OutOfMemory when they do not fit).
+void* rows_alloc(size_t bytes, cudaStream_t s, const char* what);
+
 struct Run {
   int dtype = 0;  // 0 float32, 1 float64
   int device = 0;
@@ -78,8 +87,8 @@ struct Run {
   int32_t rows = 1, rows_cap = 0, K = 0;
   std::vector<int32_t> n_imfs, error, hist_scale, hist_sifts;
   std::vector<double> hist_spacing, hist_energy;
-  void* dev_rows = nullptr;  // cudaMalloc'd
-  void* dev_orient = nullptr;  // (B, cap - 1, D + 1, count) with Params::orientation, cudaMalloc'd
+  void* dev_rows = nullptr;  // from the device's rows pool (rows_alloc)
+  void* dev_orient = nullptr;  // (B, cap - 1, D + 1, count) with Params::orientation, rows pool
   ~Run();
   // (B, P, count) into dst: NaN rows for failed elements, zeros above an element's residue.
   void collect(void* dst, bool dst_on_device, cudaStream_t s);

@@ -15,11 +15,10 @@ namespace {
 std::atomic<long long> g_launches{0};
 std::atomic<bool> g_on{false};
 std::mutex g_mu;
-struct Pair {
-  cudaEvent_t a, b;
-};
-std::vector<Pair> g_events;
-cudaEvent_t g_open = nullptr;
+// Events are created once and reused across eda_profile resets (no event creation inside a timed
+// region once the pool holds enough): launch i uses events 2 i and 2 i + 1.
+std::vector<cudaEvent_t> g_pool;
+size_t g_used = 0;
 __device__ unsigned long long g_cube_bytes;
 
 }  // namespace
@@ -38,15 +37,14 @@ unsigned long long* cube_bytes_counter() {
 void profile_cube_launch(cudaStream_t s, bool begin) {
   if (!profiling()) return;
   std::lock_guard<std::mutex> lock(g_mu);
-  cudaEvent_t e;
-  EDAB_CUDA(cudaEventCreate(&e));
-  EDAB_CUDA(cudaEventRecord(e, s));
-  if (begin) {
-    g_open = e;
-  } else {
-    g_events.push_back(Pair{g_open, e});
-    g_open = nullptr;
+  if (!begin && g_used % 2 == 0) return;  // an end without its begin
+  if (begin && g_used % 2 == 1) --g_used;  // a begin whose launch failed before its end
+  if (g_used == g_pool.size()) {
+    cudaEvent_t e;
+    EDAB_CUDA(cudaEventCreate(&e));
+    g_pool.push_back(e);
   }
+  EDAB_CUDA(cudaEventRecord(g_pool[g_used++], s));
 }
 
 }  // namespace edab
@@ -57,11 +55,13 @@ extern "C" {
 EDA_API int eda_profile(int enable) {
   try {
     std::lock_guard<std::mutex> lock(edab::g_mu);
-    for (const auto& p : edab::g_events) {
-      cudaEventDestroy(p.a);
-      cudaEventDestroy(p.b);
+    edab::g_used = 0;
+    // enough events for a long timed region, made before it starts
+    while (enable && edab::g_pool.size() < 4096) {
+      cudaEvent_t e;
+      EDAB_CUDA(cudaEventCreate(&e));
+      edab::g_pool.push_back(e);
     }
-    edab::g_events.clear();
     edab::g_launches.store(0);
     const unsigned long long zero = 0;
     EDAB_CUDA(cudaMemcpyToSymbol(edab::g_cube_bytes, &zero, sizeof zero));
@@ -79,15 +79,16 @@ EDA_API int eda_profile_read(int64_t* launches, int64_t* cube_launches, double* 
     EDAB_CUDA(cudaDeviceSynchronize());
     std::lock_guard<std::mutex> lock(edab::g_mu);
     double ms = 0.0;
-    for (const auto& p : edab::g_events) {
+    const size_t pairs = edab::g_used / 2;
+    for (size_t i = 0; i < pairs; ++i) {
       float t = 0.f;
-      EDAB_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
+      EDAB_CUDA(cudaEventElapsedTime(&t, edab::g_pool[2 * i], edab::g_pool[2 * i + 1]));
       ms += t;
     }
     unsigned long long bytes = 0;
     EDAB_CUDA(cudaMemcpyFromSymbol(&bytes, edab::g_cube_bytes, sizeof bytes));
     if (launches) *launches = edab::g_launches.load();
-    if (cube_launches) *cube_launches = static_cast<int64_t>(edab::g_events.size());
+    if (cube_launches) *cube_launches = static_cast<int64_t>(pairs);
     if (cube_bytes) *cube_bytes = static_cast<double>(bytes);
     if (cube_ms) *cube_ms = ms;
     return EDA_OK;

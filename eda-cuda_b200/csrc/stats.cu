@@ -360,7 +360,10 @@ __global__ void __launch_bounds__(kThreads) sel_pick(const int32_t* run, SelStat
   }
 }
 
-__global__ void sel_final(int64_t B, const int32_t* run, const SelState* st, double q, double* out, int64_t* count) {
+// low: key bits below the last digit the passes resolved; every item sharing the resolved prefix
+// has the same low bits (float values: zeros for keys of non-negative values, ones for negative).
+__global__ void sel_final(int64_t B, const int32_t* run, const SelState* st, double q, double* out, int64_t* count,
+                          int32_t low) {
   const int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (b >= B || (run && !run[b])) return;
   const SelState S = st[b];
@@ -369,8 +372,9 @@ __global__ void sel_final(int64_t B, const int32_t* run, const SelState* st, dou
     out[b] = d_nan();
     return;
   }
-  const double a = sel_value(S.prefix[0]);
-  const double c = sel_value(S.prefix[1]);
+  const uint64_t lm = low > 0 ? (1ULL << low) - 1ULL : 0ULL;
+  const double a = sel_value(S.prefix[0] | ((S.prefix[0] >> 63) ? 0ULL : lm));
+  const double c = sel_value(S.prefix[1] | ((S.prefix[1] >> 63) ? 0ULL : lm));
   if (q < 0) out[b] = S.count % 2 ? a : (a + c) / 2.0;
   else out[b] = q_lerp(a, c, S.gamma);
 }
@@ -433,7 +437,11 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
   int64_t nblk = (a.items + int64_t{kThreads} * 32 - 1) / (int64_t{kThreads} * 32);
   nblk = std::clamp<int64_t>(nblk, 1, 1024);
   if (B > 65535) throw std::invalid_argument("edab: select batch too large");
-  for (int p = 0; p < kSelPasses; ++p) {
+  // float items (a float32 field or its float32 differences, no centre) have double keys whose low
+  // 29 bits depend only on the sign: four passes resolve every bit above bit 20
+  const int passes = std::is_same_v<T, float> && sel.center == nullptr ? 4 : kSelPasses;
+  int low = 0;
+  for (int p = 0; p < passes; ++p) {
     const int top = 64 - kSelBits * p;
     const int shift = top - kSelBits > 0 ? top - kSelBits : 0;
     const int width = top - shift;
@@ -442,8 +450,9 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
     EDAB_LAUNCH("sel_hist");
     sel_pick<<<static_cast<unsigned>(B), kThreads, 0, s>>>(run, st, hist, shift, width, p == 0, q);
     EDAB_LAUNCH("sel_pick");
+    low = shift;
   }
-  sel_final<<<blocks_for(B), kThreads, 0, s>>>(B, run, st, q, out, count);
+  sel_final<<<blocks_for(B), kThreads, 0, s>>>(B, run, st, q, out, count, low);
   EDAB_LAUNCH("sel_final");
 }
 
@@ -591,6 +600,8 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   // the run of samples equal to x[s] from s (s a run start): significant extremum -> flag its peak
   const auto visit = [&](int p, int32_t s) {
     const T* x = X + p * LX;
+    // the threshold at s, read for every sample (coalesced over the warp) ahead of its use at a peak
+    const T tp_s = tau[eoff + base_s[p] + s * step];
     const T cur = xs(x, s), prev = xs(x, s - 1);
     if (!(prev < cur || prev > cur)) return;
     const T* pmin = bmin + p * nb;
@@ -620,7 +631,7 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
     if (!is_max && !is_min) return;
     const int32_t pk = (s + e) / 2;
     const int64_t at = eoff + base_s[p] + pk * step;
-    const T tp = tau[at];
+    const T tp = pk == s ? tp_s : tau[at];
     const bool sig = is_max ? side_deep<true, -1>(x, n, pk, cur, tp, pmin, pmax) && side_deep<true, 1>(x, n, pk, cur, tp, pmin, pmax)
                             : side_deep<false, -1>(x, n, pk, cur, tp, pmin, pmax) && side_deep<false, 1>(x, n, pk, cur, tp, pmin, pmax);
     if (sig) {
@@ -634,10 +645,12 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
       for (int32_t s = 1 + threadIdx.x; s <= n - 2; s += blockDim.x) visit(p, s);
     }
   } else {
-    const int p = threadIdx.x & 31;
-    const int32_t nw = static_cast<int32_t>(blockDim.x >> 5);
-    if (p < P && ok_s[p]) {
-      for (int32_t s = 1 + static_cast<int32_t>(threadIdx.x >> 5); s <= n - 2; s += nw) visit(p, s);
+    // lanes over the panel's columns; a warp covers 32 / P rows (P a power of two <= 32)
+    const int p = threadIdx.x & (P - 1);
+    const int32_t rpw = 32 / P;
+    const int32_t nrows = static_cast<int32_t>(blockDim.x >> 5) * rpw;
+    if (ok_s[p]) {
+      for (int32_t s = 1 + static_cast<int32_t>(threadIdx.x / P); s <= n - 2; s += nrows) visit(p, s);
     }
   }
   for (int d = 16; d > 0; d >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, d);
@@ -700,10 +713,10 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
     const int32_t nb = (n + kBlk - 1) / kBlk;
     int P;
     if (a == g.dim - 1) P = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({static_cast<int64_t>(8192 / n), g.rows, 64})));
-    else P = static_cast<int>(std::min<int64_t>(32, g.stride[a]));
+    else P = static_cast<int>(std::min<int64_t>(16, g.stride[a]));  // a power of two (stride: a multiple of 32)
     const int32_t LX = (n + ((n - 1) >> 5) + 1) | 1;  // padded line words, odd
     const auto bytes = [&](int p) { return static_cast<size_t>(p) * (LX + 2 * nb) * sizeof(T); };
-    while (P > 1 && bytes(P) > cap) --P;
+    while (P > 1 && bytes(P) > cap) P = a == g.dim - 1 ? P - 1 : P / 2;
     if (bytes(P) > cap) throw std::invalid_argument("edab: a line exceeds the shared memory of the extrema pass");
     int64_t groups;
     if (a == g.dim - 1) {
