@@ -334,25 +334,40 @@ struct SegPoint {
   int32_t off0[D], off1[D];
   T w0[D], w1[D];
 };
+// reflect_any for 32-bit indices (|i| < 2^30, n <= 8192)
+__device__ __forceinline__ int32_t reflect32(int32_t i, int32_t n) {
+  if (i >= 0 && i < n) return i;
+  if (i < 0 && i >= -n) return -i - 1;
+  if (i >= n && i < 2 * n) return 2 * n - 1 - i;
+  int32_t m = i % (2 * n);
+  if (m < 0) m += 2 * n;
+  return m < n ? m : 2 * n - 1 - m;
+}
+// xd: the voxel's coordinates as doubles (converted once per voxel).
 template <class T, int D>
-__device__ __forceinline__ SegPoint<T, D> seg_point(const Geom& g, const int32_t* x, const double* ov, int q) {
+__device__ __forceinline__ SegPoint<T, D> seg_point(const Geom& g, const double* xd, const double* ov, int q) {
   SegPoint<T, D> P;
-  const double s = static_cast<double>(q / 2 + 1) / 2.0;
+  const double s = (q >> 1) ? 1.0 : 0.5;  // (q / 2 + 1) / 2
   const int sg = q & 1;
 #pragma unroll
   for (int a = 0; a < D; ++a) {
     const double off = __dmul_rn(s, ov[a]);
-    const double xa = static_cast<double>(x[a]);
-    const double y = sg == 0 ? __dadd_rn(xa, off) : __dsub_rn(xa, off);
+    const double y = sg == 0 ? __dadd_rn(xd[a], off) : __dsub_rn(xd[a], off);
     const double fl = floor(y);
     const double tt = __dsub_rn(y, fl);
-    const int64_t i0 = static_cast<int64_t>(fl);
     const T t1 = static_cast<T>(tt);
     P.w1[a] = t1;
     P.w0[a] = sub_rn(T(1), t1);
-    const int64_t st = a == D - 1 ? 1 : g.stride[a];
-    P.off0[a] = static_cast<int32_t>(reflect_any(i0, g.n[a]) * st);
-    P.off1[a] = static_cast<int32_t>(reflect_any(i0 + 1, g.n[a]) * st);
+    const int32_t st = a == D - 1 ? 1 : static_cast<int32_t>(g.stride[a]);  // offsets stay below 2^31
+    if (fabs(fl) < 1073741824.0) {
+      const int32_t i0 = static_cast<int32_t>(fl);
+      P.off0[a] = reflect32(i0, g.n[a]) * st;
+      P.off1[a] = reflect32(i0 + 1, g.n[a]) * st;
+    } else {
+      const int64_t i0 = static_cast<int64_t>(fl);
+      P.off0[a] = static_cast<int32_t>(reflect_any(i0, g.n[a]) * st);
+      P.off1[a] = static_cast<int32_t>(reflect_any(i0 + 1, g.n[a]) * st);
+    }
   }
   return P;
 }
@@ -418,13 +433,15 @@ __global__ void __launch_bounds__(kThreads, 4) gather_kernel(Geom g, const Elem*
         const bool pts0 = use0 && ((pts_mask >> l) & 1u);
         const bool pts1 = use1 && ((pts_mask >> (l + 1)) & 1u);
         if (pts0 || pts1) {
-          double ov[D];
+          double ov[D], xd[D];
           ov[0] = static_cast<double>(__ldg(o0 + at));
           ov[1] = static_cast<double>(__ldg(o1 + at));
           if constexpr (D >= 3) ov[2] = static_cast<double>(__ldg(o2 + at));
+#pragma unroll
+          for (int a = 0; a < D; ++a) xd[a] = static_cast<double>(x[a]);
 #pragma unroll 1
           for (int q = 0; q < 4; ++q) {
-            const SegPoint<T, D> P = seg_point<T, D>(g, x, ov, q);
+            const SegPoint<T, D> P = seg_point<T, D>(g, xd, ov, q);
             if (pts0) {
               a00 = gather_op<OP>(a00, interp_read<T, D>(fa0, P), false);
               if constexpr (OP == 2) a01 = gather_op<OP>(a01, interp_read<T, D>(fa1, P), true);
