@@ -79,6 +79,38 @@ int eda_decompose(const void* x, int x_on_device, int dtype, int dim, int64_t ba
   });
 }
 
+int eda_decompose_strided(const void* x, const eda_source* src, int dtype, int dim, const int64_t* n,
+                          const eda_params* params, void* stream, eda_run** out) {
+  return guarded([&] {
+    if (!out || !n || !params || !src) throw std::invalid_argument("eda: null argument");
+    if (dim < 1 || dim > edab::kMaxDim) throw std::invalid_argument("eda: D must be 1, 2 or 3");
+    if (src->batch_axes < 0 || src->batch_axes > edab::kMaxBatchAxes) {
+      throw std::invalid_argument("eda: at most 64 batch axes");
+    }
+    if (!src->stride || (src->batch_axes > 0 && (!src->batch_shape || !src->batch_stride))) {
+      throw std::invalid_argument("eda: null layout array");
+    }
+    edab::SourceView v;
+    v.type = src->type;
+    v.batch_axes = src->batch_axes;
+    for (int k = 0; k < src->batch_axes; ++k) {
+      v.batch_shape[k] = src->batch_shape[k];
+      v.batch_stride[k] = src->batch_stride[k];
+    }
+    for (int a = 0; a < dim; ++a) v.stride[a] = src->stride[a];
+    edab::Params p;
+    p.max_imf = params->max_imf;
+    p.tie_tolerance = params->tie_tolerance;
+    p.sifts = params->sifts;
+    p.check_finite = params->check_finite != 0;
+    p.max_chunk = params->max_chunk;
+    p.orientation = params->orientation != 0;
+    auto r = std::make_unique<eda_run>();
+    r->run = edab::decompose_strided(x, v, dtype, dim, n, p, static_cast<cudaStream_t>(stream));
+    *out = r.release();
+  });
+}
+
 int eda_decompose_ragged(const void* const* x, int x_on_device, int dtype, int dim, int64_t count, const int64_t* n,
                          const eda_params* params, int32_t workers, void* stream, eda_ragged_run** out) {
   return guarded([&] {

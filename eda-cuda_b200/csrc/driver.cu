@@ -342,8 +342,12 @@ void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params&
   if (p.max_chunk < 0) throw std::invalid_argument("eda: max_chunk must be >= 0");
 }
 
-std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
-                               const Params& p, cudaStream_t s) {
+namespace {
+
+// decompose() and decompose_strided(): src (device input only) gives the input's own layout and
+// element type, converted chunk by chunk into the staging buffer; without it x is dense.
+std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceView* src, int dtype, int dim,
+                                    int64_t batch, const int64_t* n, const Params& p, cudaStream_t s) {
   validate(dtype, dim, batch, n, p);
   const bool f32 = dtype == 0;
   const size_t es = f32 ? 4 : 8;
@@ -416,9 +420,14 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
     ws.reset();
     // the chunk's dense input, staged at the head of the workspace
     void* staged = ws.take<unsigned char>(static_cast<size_t>(nb) * static_cast<size_t>(g.count) * es);
-    const unsigned char* src = static_cast<const unsigned char*>(x) + static_cast<size_t>(b0) * g.count * es;
-    EDAB_CUDA(cudaMemcpyAsync(staged, src, static_cast<size_t>(nb) * g.count * es,
-                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    if (src) {
+      if (f32) convert_chunk<float>(s, *src, x, b0, nb, dim, n, static_cast<float*>(staged));
+      else convert_chunk<double>(s, *src, x, b0, nb, dim, n, static_cast<double*>(staged));
+    } else {
+      const unsigned char* in = static_cast<const unsigned char*>(x) + static_cast<size_t>(b0) * g.count * es;
+      EDAB_CUDA(cudaMemcpyAsync(staged, in, static_cast<size_t>(nb) * g.count * es,
+                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    }
     const size_t ho = static_cast<size_t>(b0) * static_cast<size_t>(cap - 1);
     unsigned char* rows0 = static_cast<unsigned char*>(run->dev_rows) + static_cast<size_t>(b0) * cap * g.count * es;
     unsigned char* orient0 =
@@ -476,6 +485,28 @@ std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim
     for (int32_t j = 0; j < run->n_imfs[static_cast<size_t>(b)]; ++j) e[j] = std::ldexp(e[j], 2 * k);
   }
   return run;
+}
+
+}  // namespace
+
+std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
+                               const Params& p, cudaStream_t s) {
+  return decompose_impl(x, on_device, nullptr, dtype, dim, batch, n, p, s);
+}
+
+std::unique_ptr<Run> decompose_strided(const void* x, const SourceView& src, int dtype, int dim, const int64_t* n,
+                                       const Params& p, cudaStream_t s) {
+  (void)source_item_size(src.type);  // rejects an unknown element type
+  if (src.batch_axes < 0 || src.batch_axes > kMaxBatchAxes) {
+    throw std::invalid_argument("eda: at most " + std::to_string(kMaxBatchAxes) + " batch axes");
+  }
+  int64_t batch = 1;
+  for (int k = 0; k < src.batch_axes; ++k) {
+    if (src.batch_shape[k] < 0) throw std::invalid_argument("eda: a batch extent is negative");
+    batch *= src.batch_shape[k];
+  }
+  if (batch > 0 && !x) throw std::invalid_argument("eda: null input");
+  return decompose_impl(x, true, &src, dtype, dim, batch, n, p, s);
 }
 
 }  // namespace edab

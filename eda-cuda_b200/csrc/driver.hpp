@@ -118,6 +118,27 @@ std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_devic
 // the current device, on stream s. Throws std::invalid_argument, OutOfMemory or CudaError.
 std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
                                const Params& p, cudaStream_t s);
+
+// A device input read where it lies: element type (the C ABI's EDA_SRC_* codes), batch axes (C
+// order) and strides in elements of that type, of either sign.
+constexpr int kSrcBool = 0, kSrcI8 = 1, kSrcI16 = 2, kSrcI32 = 3, kSrcI64 = 4, kSrcU8 = 5, kSrcU16 = 6, kSrcU32 = 7,
+              kSrcU64 = 8, kSrcF16 = 9, kSrcBF16 = 10, kSrcF32 = 11, kSrcF64 = 12;
+constexpr int kMaxBatchAxes = 64;
+struct SourceView {
+  int32_t type = kSrcF32;
+  int32_t batch_axes = 0;
+  int64_t batch_shape[kMaxBatchAxes] = {};
+  int64_t batch_stride[kMaxBatchAxes] = {};
+  int64_t stride[kMaxDim] = {};
+};
+size_t source_item_size(int type);
+// dst (nb, count) dense <- elements b0 .. b0 + nb - 1 of x (src's layout), cast to T, on stream s.
+template <class T>
+void convert_chunk(cudaStream_t s, const SourceView& src, const void* x, int64_t b0, int64_t nb, int dim,
+                   const int64_t* n, T* dst);
+// decompose() of a device input in any layout and element type (converted chunk by chunk).
+std::unique_ptr<Run> decompose_strided(const void* x, const SourceView& src, int dtype, int dim, const int64_t* n,
+                                       const Params& p, cudaStream_t s);
 void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params& p);
 
 // eda.monogenic of the batch x (host or current device, C-contiguous (batch, n..)): out (host or

@@ -219,7 +219,14 @@ def decompose(
         torch = _device._torch()
         tdt = getattr(torch, target)
         t = data.permute(order) if order != list(range(ndim)) else data
-        t = t.to(tdt).contiguous().reshape((B,) + spatial)
+        layout = None
+        if t.dtype == tdt and t.is_contiguous():
+            t = t.reshape((B,) + spatial)  # read in place
+        else:
+            # any other element type or layout: the engine gathers and casts each chunk itself
+            # (cpp/src/field/convert.cu:69-170 of the reference), no converted copy of x is made
+            layout = (src, batch_shape, tuple(int(data.stride(i)) for i in batch_axes),
+                      tuple(int(data.stride(a)) for a in axes))
         dev = t.device
         if B == 0:
             rows_t, raw = torch.zeros((0, 1) + spatial, dtype=tdt, device=dev), core._empty_info(0)
@@ -238,7 +245,7 @@ def decompose(
 
                 rows_t, raw = core.decompose_device(t.data_ptr(), dev.index or 0, target, (B,) + spatial, max_imf,
                                                     tie, sifts, check_finite, 0, st.cuda_stream, alloc,
-                                                    orient_of if return_orientation else None)
+                                                    orient_of if return_orientation else None, layout)
     else:
         xc = data if data.dtype == np.dtype(target) else data.astype(target)
         xt = np.ascontiguousarray(xc.transpose(order)) if order != list(range(ndim)) else xc
@@ -470,7 +477,14 @@ def monogenic(
         torch = _device._torch()
         tdt = getattr(torch, target)
         t = data.permute(order) if order != list(range(ndim)) else data
-        t = t.to(tdt).contiguous().reshape((B,) + spatial)
+        layout = None
+        if t.dtype == tdt and t.is_contiguous():
+            t = t.reshape((B,) + spatial)  # read in place
+        else:
+            # any other element type or layout: the engine gathers and casts each chunk itself
+            # (cpp/src/field/convert.cu:69-170 of the reference), no converted copy of x is made
+            layout = (src, batch_shape, tuple(int(data.stride(i)) for i in batch_axes),
+                      tuple(int(data.stride(a)) for a in axes))
         dev = t.device
         flat = torch.empty(planes * B * count, dtype=tdt, device=dev)
         if B:

@@ -35,6 +35,19 @@ class _Params(ctypes.Structure):
     ]
 
 
+class _Source(ctypes.Structure):
+    """eda_source: a device input's element type and layout (strides in elements, either sign)."""
+
+    _fields_ = [("type", ctypes.c_int32), ("batch_axes", ctypes.c_int32),
+                ("batch_shape", ctypes.POINTER(ctypes.c_int64)), ("batch_stride", ctypes.POINTER(ctypes.c_int64)),
+                ("stride", ctypes.POINTER(ctypes.c_int64))]
+
+
+# EDA_SRC_* codes of include/eda_b200.h
+SOURCE_TYPES = {"bool": 0, "int8": 1, "int16": 2, "int32": 3, "int64": 4, "uint8": 5, "uint16": 6, "uint32": 7,
+                "uint64": 8, "float16": 9, "bfloat16": 10, "float32": 11, "float64": 12}
+
+
 class Core:
     """The engine's entry points with the reference extension's Python signatures."""
 
@@ -43,6 +56,8 @@ class Core:
         vp, i32, i64, f64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
         L.eda_decompose.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, i64, ctypes.POINTER(i64),
                                     ctypes.POINTER(_Params), vp, ctypes.POINTER(vp)]
+        L.eda_decompose_strided.argtypes = [vp, ctypes.POINTER(_Source), ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(i64), ctypes.POINTER(_Params), vp, ctypes.POINTER(vp)]
         L.eda_run_shape.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i32),
                                     ctypes.POINTER(i64), ctypes.POINTER(i64)]
         L.eda_run_info.argtypes = [vp] + [vp] * 6
@@ -102,15 +117,25 @@ class Core:
     # -- the decomposition ---------------------------------------------------------------------
     def _run(self, ptr: int, on_device: bool, dtype: np.dtype, shape: tuple[int, ...], max_imf: int,
              tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int, stream: int,
-             orientation: bool = False):
+             orientation: bool = False, layout=None):
         p = _Params(int(max_imf), -1.0 if tie_tolerance is None else float(tie_tolerance), int(sifts),
                     int(bool(check_finite)), int(max_chunk), int(bool(orientation)))
         n = (ctypes.c_int64 * 3)(*[int(v) for v in shape[1:]], *([1] * (4 - len(shape))))
         run = ctypes.c_void_p()
         code = 0 if dtype == np.float32 else 1
-        self._check(self._lib.eda_decompose(ctypes.c_void_p(ptr), int(on_device), code, len(shape) - 1,
-                                            int(shape[0]), n, ctypes.byref(p), ctypes.c_void_p(stream),
-                                            ctypes.byref(run)))
+        if layout is None:
+            self._check(self._lib.eda_decompose(ctypes.c_void_p(ptr), int(on_device), code, len(shape) - 1,
+                                                int(shape[0]), n, ctypes.byref(p), ctypes.c_void_p(stream),
+                                                ctypes.byref(run)))
+            return run
+        src_type, batch_shape, batch_stride, stride = layout
+        k = len(batch_shape)
+        bs = (ctypes.c_int64 * max(k, 1))(*[int(v) for v in batch_shape])
+        bt = (ctypes.c_int64 * max(k, 1))(*[int(v) for v in batch_stride])
+        st = (ctypes.c_int64 * 3)(*[int(v) for v in stride], *([0] * (3 - len(stride))))
+        src = _Source(SOURCE_TYPES[src_type], k, bs, bt, st)
+        self._check(self._lib.eda_decompose_strided(ctypes.c_void_p(ptr), ctypes.byref(src), code, len(shape) - 1,
+                                                    n, ctypes.byref(p), ctypes.c_void_p(stream), ctypes.byref(run)))
         return run
 
     def _info(self, run) -> tuple[dict, int, int, int]:
@@ -174,14 +199,16 @@ class Core:
 
     def decompose_device(self, ptr: int, device: int, dtype: str, shape: tuple[int, ...], max_imf: int,
                          tie_tolerance: float | None, sifts: int, check_finite: bool, max_chunk: int,
-                         stream: int, out_ptr_of, orient_of=None) -> tuple:
+                         stream: int, out_ptr_of, orient_of=None, layout=None) -> tuple:
         """Decomposes the C-contiguous device array at ptr (B, *spatial) in the compute dtype on its
-        device; ``out_ptr_of(P)`` allocates the (B, P, *spatial) output and returns it with its
-        pointer; with ``orient_of`` (return_orientation), ``orient_of(K)`` allocates the direction
+        device, or with ``layout`` = (source dtype name, batch shape, batch strides, spatial strides;
+        strides in elements) the array at ptr in that layout, converted by the engine chunk by chunk;
+        ``out_ptr_of(P)`` allocates the (B, P, *spatial) output and returns it with its pointer; with
+        ``orient_of`` (return_orientation), ``orient_of(K)`` allocates the direction
         (B, K, D, *spatial) and coherence (B, K, *spatial) outputs and returns them with their
         pointers, kept in info["direction"] / info["coherence"]."""
         run = self._run(ptr, True, np.dtype(dtype), shape, max_imf, tie_tolerance, sifts, check_finite,
-                        max_chunk, stream, orient_of is not None)
+                        max_chunk, stream, orient_of is not None, layout)
         try:
             info, P, B, count = self._info(run)
             out, out_ptr = out_ptr_of(P)

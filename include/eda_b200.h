@@ -67,6 +67,42 @@ typedef struct eda_run eda_run;
 EDA_API int eda_decompose(const void* x, int x_on_device, int dtype, int dim, int64_t batch, const int64_t* n,
                   const eda_params* params, void* stream, eda_run** out);
 
+/* Element types of a device input that eda_decompose_strided reads where it lies (the reference's
+ * SourceType, cpp/src/field/convert.hpp:18). */
+#define EDA_SRC_BOOL 0
+#define EDA_SRC_INT8 1
+#define EDA_SRC_INT16 2
+#define EDA_SRC_INT32 3
+#define EDA_SRC_INT64 4
+#define EDA_SRC_UINT8 5
+#define EDA_SRC_UINT16 6
+#define EDA_SRC_UINT32 7
+#define EDA_SRC_UINT64 8
+#define EDA_SRC_FLOAT16 9
+#define EDA_SRC_BFLOAT16 10
+#define EDA_SRC_FLOAT32 11
+#define EDA_SRC_FLOAT64 12
+
+/* The layout of a device input (the reference's SourceLayout, cpp/src/field/convert.hpp:28-36):
+ * element (j, i_0..i_{dim-1}) lies at x + sum_k j_k batch_stride[k] + sum_a i_a stride[a], with
+ * j_0..j_{batch_axes-1} the C-order multi-index of batch element j over batch_shape; strides in
+ * elements of the source type, either sign; at most 64 batch axes (none: one element). */
+typedef struct eda_source {
+  int32_t type;                 /* EDA_SRC_* */
+  int32_t batch_axes;
+  const int64_t* batch_shape;   /* [batch_axes] */
+  const int64_t* batch_stride;  /* [batch_axes] */
+  const int64_t* stride;        /* [dim] */
+} eda_source;
+
+/* eda_decompose of a CUDA input on the current device in any layout and element type: each chunk
+ * is gathered and cast to dtype (round to nearest even; bool to 0 / 1) by one kernel into the
+ * chunk's staging buffer, with no converted copy of the whole input. The batch is the product of
+ * batch_shape. Replaces the strided gather and cast of the reference's decompose_device
+ * (cpp/src/field/convert.cu:69-170, cpp/python/decompose.cpp:25-82). */
+EDA_API int eda_decompose_strided(const void* x, const eda_source* src, int dtype, int dim, const int64_t* n,
+                                  const eda_params* params, void* stream, eda_run** out);
+
 /* The shape of a run: batch, P (the output rows per element: one more than the largest IMF count
  * of the elements without an error), K (the largest IMF count: the width of the information
  * arrays), the samples per element and the elements per chunk (cpp/python/decompose.cpp:188-214). */
