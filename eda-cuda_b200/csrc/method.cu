@@ -396,7 +396,7 @@ __device__ __forceinline__ T gather_op(T acc, T v, bool second) {
 }
 
 template <class T, int D, int OP>
-__global__ void __launch_bounds__(kThreads, 4) gather_kernel(Geom g, const Elem* __restrict__ el,
+__global__ void __launch_bounds__(kThreads, 6) gather_kernel(Geom g, const Elem* __restrict__ el,
                                                          const int32_t* __restrict__ run, const uint8_t* __restrict__ lo,
                                                          const T* __restrict__ t, const T* __restrict__ o0,
                                                          const T* __restrict__ o1, const T* __restrict__ o2,
