@@ -29,7 +29,7 @@ void Workspace::release() {
   used_ = 0;
 }
 
-void Workspace::reserve(size_t bytes) {
+void Workspace::reserve(size_t bytes, cudaStream_t s) {
   int dev = 0;
   EDAB_CUDA(cudaGetDevice(&dev));
   if (base_ && size_ >= bytes && dev == device_) return;
@@ -41,8 +41,8 @@ void Workspace::reserve(size_t bytes) {
     throw OutOfMemory("eda: the workspace (" + std::to_string(bytes >> 20) + " MiB) does not fit the device memory");
   }
   EDAB_CUDA(e);
-  // deterministic contents: pad samples of every field start at zero
-  EDAB_CUDA(cudaMemset(p, 0, bytes));
+  // deterministic contents: pad samples of every field start at zero (ordered on the caller's stream)
+  EDAB_CUDA(cudaMemsetAsync(p, 0, bytes, s));
   base_ = static_cast<unsigned char*>(p);
   size_ = bytes;
   device_ = dev;
@@ -410,7 +410,7 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
     Bc = (Bc + 1) / 2;
   }
   run->chunk = Bc;
-  ws.reserve(need(Bc));
+  ws.reserve(need(Bc), s);
   std::vector<Elem> elems(static_cast<size_t>(batch));
   std::vector<int32_t> exps(static_cast<size_t>(batch), 0);
   std::vector<Elem> part;

@@ -19,7 +19,10 @@ class Workspace {
   Workspace(void* external, size_t bytes)
       : base_(static_cast<unsigned char*>(external)), size_(bytes), owned_(false) {}
   ~Workspace();
-  void reserve(size_t bytes);  // frees and reallocates when the buffer is smaller
+  // frees and reallocates when the buffer is smaller; a new buffer is zeroed on stream s (the
+  // caller's stream, which may be a non-blocking one: a legacy-stream memset would not be ordered
+  // before the caller's work on it)
+  void reserve(size_t bytes, cudaStream_t s);
   void reset() { used_ = 0; }
   template <class T>
   T* take(size_t count) {

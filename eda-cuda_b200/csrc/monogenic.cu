@@ -84,7 +84,7 @@ void run_monogenic(const void* x, bool on_device, int dim, int64_t batch, const 
   const size_t margin = std::max<size_t>(size_t{256} << 20, free_b / 20);
   Workspace& ws = thread_workspace();
   while (Bc > 1 && need(Bc) + margin > free_b) Bc = (Bc + 1) / 2;
-  ws.reserve(need(Bc));
+  ws.reserve(need(Bc), s);
   const OrientPlan& plan = orient_plan(g, std::is_same_v<T, double>);
   std::vector<int32_t> bad(static_cast<size_t>(Bc));
   for (int64_t b0 = 0; b0 < batch; b0 += Bc) {

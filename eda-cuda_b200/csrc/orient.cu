@@ -432,6 +432,9 @@ const OrientPlan& orient_plan(const Geom& g, bool f64) {
     if (f64) upload_axis<double>(*p, a, g.n[a]);
     else upload_axis<float>(*p, a, g.n[a]);
   }
+  // the uploads above are legacy-stream copies from pageable memory, which may return before the
+  // data lands: complete them before any stream (a non-blocking one included) reads the plan
+  EDAB_CUDA(cudaStreamSynchronize(nullptr));
   const OrientPlan& ref = *p;
   cache.emplace(key, std::move(p));
   return ref;

@@ -65,6 +65,7 @@ EDA_API int eda_profile(int enable) {
     edab::g_launches.store(0);
     const unsigned long long zero = 0;
     EDAB_CUDA(cudaMemcpyToSymbol(edab::g_cube_bytes, &zero, sizeof zero));
+    EDAB_CUDA(cudaDeviceSynchronize());  // the reset lands before work on any stream counts
     edab::g_on.store(enable != 0);
     return EDA_OK;
   } catch (...) {

@@ -119,3 +119,30 @@ def test_ragged_rejects_a_field_beyond_the_axis_limit(torch):
 
     with pytest.raises(ValueError, match="exceeds the limit"):
         eda.decompose_ragged([signal(300, 1).astype(np.float32), signal(8193, 2).astype(np.float32)])
+
+
+def test_fresh_workspaces_are_zeroed_on_the_workers_streams(torch):
+    """Each ragged call starts new worker threads, whose workspaces are allocated and zeroed anew.
+    With the caller on a non-blocking stream and the legacy default stream kept busy by other work,
+    a zeroing queued on the legacy stream would land in the middle of the workers' kernels (which
+    run on their own non-blocking streams) and corrupt their inputs; zeroed on the workers' own
+    streams, every field must still equal its one-field call."""
+    import eda
+
+    xs = [signal(400, 11), signal(400, 13), signal(520, 12), signal(520, 14)]
+    wants = [alone(eda, x) for x in xs]
+    xd = [torch.from_numpy(x).cuda() for x in xs]  # device fields: the workers follow the caller's stream
+    side = torch.cuda.Stream()
+    a = torch.randn(8192, 8192, device="cuda")
+    for _ in range(3):
+        torch.cuda.synchronize()
+        busy = a
+        for _ in range(24):  # tens of milliseconds of work on the legacy default stream
+            busy = busy @ a
+        with torch.cuda.stream(side):
+            rows, infos = eda.decompose_ragged(xd, workers=2, return_info=True, errors="status")
+            side.synchronize()
+        for i, (want, winfo, k) in enumerate(wants):
+            assert same(np.asarray(rows[i]), np.asarray(want)), i
+            assert int(infos[i].n_imfs) == int(winfo.n_imfs[0])
+    torch.cuda.synchronize()
