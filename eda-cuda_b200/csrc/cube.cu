@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxGroupsPerCta = 8;  // line groups one CTA runs at most
+constexpr int kMaxGroupsPerCta = 1;  // line groups one CTA runs at most (measured: 1 is fastest)
 
 __host__ __device__ constexpr int32_t tot_slots(int32_t n) { return n / 8 + 24; }
 // Line stride of the row layout in elements: the padded row rounded up, plus 16 bytes (4 words
