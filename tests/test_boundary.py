@@ -117,3 +117,32 @@ def test_ragged_empty_batch():
 
     assert eda.decompose_ragged([]) == []
     assert eda.decompose_ragged([], return_info=True) == ([], [])
+
+
+@pytest.mark.parametrize("case,message", [
+    ("type", "unknown source element type"),
+    ("axes", "at most 64 batch axes"),
+    ("dim", "D must be 1, 2 or 3"),
+    ("null", "null"),
+    ("extent", "batch extent is negative"),
+])
+def test_strided_argument_rules(case, message):
+    """eda_decompose_strided rejects a bad layout before it touches the device."""
+    from eda import _native
+
+    core = _native.core()
+    lib = core._lib
+    shape = (ctypes.c_int64 * 1)(-1 if case == "extent" else 2)
+    bstride = (ctypes.c_int64 * 1)(64)
+    stride = (ctypes.c_int64 * 3)(8, 1, 0)
+    src = _native._Source(13 if case == "type" else 11, 65 if case == "axes" else 1, shape, bstride, stride)
+    n = (ctypes.c_int64 * 3)(8, 8, 1)
+    p = _native._Params(-1, -1.0, 3, 1, 0, 0)
+    run = ctypes.c_void_p()
+    src_arg = None if case == "null" else ctypes.byref(src)
+    st = lib.eda_decompose_strided(ctypes.c_void_p(1), src_arg, 0, 4 if case == "dim" else 2, n, ctypes.byref(p),
+                                   None, ctypes.byref(run))
+    assert st == 1  # EDA_INVALID_ARGUMENT
+    buf = ctypes.create_string_buffer(512)
+    lib.eda_last_error(buf, 512)
+    assert message in buf.value.decode()
