@@ -124,14 +124,31 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle(images: np.ndarray, threads: int) -> float:
-    """Seconds for the oracle to decompose `images` with `threads` host threads."""
+def cpu_oracle(images: np.ndarray, threads: int, results: list | None = None) -> float:
+    """Seconds for the oracle to decompose `images` with `threads` host threads; its (rows, info)
+    are appended to `results` when given."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
     t0 = time.perf_counter()
-    oracle.decompose(images, threads=threads)
-    return time.perf_counter() - t0
+    out = oracle.decompose(images, threads=threads)
+    secs = time.perf_counter() - t0
+    if results is not None:
+        results.append(out)
+    return secs
+
+
+def decisions_match(info, oinfo, count: int) -> int:
+    """Elements among the first `count` whose IMF count, windows and sift counts equal the oracle's."""
+    same = 0
+    for b in range(count):
+        k = int(info.n_imfs[b])
+        if k != int(oinfo["n_imfs"][b]):
+            continue
+        if (np.array_equal(np.asarray(info.windows[b][:k]), oinfo["windows"][b][:k])
+                and np.array_equal(np.asarray(info.sifts[b][:k]), oinfo["sifts"][b][:k])):
+            same += 1
+    return same
 
 
 def host_cores() -> int:
@@ -247,12 +264,22 @@ def run_ours(args) -> None:
         e2e_total = float(t.item())
     e2e = batch * world * args.steps / (e2e_total / 1000.0)
     cpu = None
+    check = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = max(1, min(host_cores(), batch))
-        secs = cpu_oracle(x_host[:threads], threads)
+        got = []
+        secs = cpu_oracle(x_host[:threads], threads, got)
         cpu = {"value": threads / secs, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{threads} of the {batch} images ({SIDE}x{SIDE} float32), one per host thread, "
                          f"{secs:.1f} s"}
+        # correctness on the benchmarked workload, outside the timed region: the decisions of the
+        # oracle's images against the engine's, and the rows of a seeded subset against the oracle
+        # run in float64
+        y_chk, info_chk = eda.decompose(x_dev[:threads], axes=(1, 2), return_info=True)
+        y_chk = y_chk.cpu().numpy() if hasattr(y_chk, "cpu") else np.asarray(y_chk)
+        n64 = min(4, threads)
+        check = {"decisions_equal": decisions_match(info_chk, got[0][1], threads), "decisions_checked": threads,
+                 "fp64_err": fp64_error([x_host[b] for b in range(n64)], [y_chk[b] for b in range(n64)], n64)}
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
@@ -281,59 +308,115 @@ def run_ours(args) -> None:
         "gpu_launches": int(launches.value),
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "parity": check,
+        "fp64_err": check["fp64_err"] if check else None,
     }
     print(json.dumps(line), flush=True)
+
+
+def signal_1d(seed: int) -> np.ndarray:
+    """The 1-D configuration: one 2048-sample float32 signal (three tones and noise), shape (1, 2048)."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(2048, dtype=np.float64)
+    x = np.sin(2 * np.pi * t / 8) + 2 * np.sin(2 * np.pi * t / 64) + 3 * np.sin(2 * np.pi * t / 512)
+    return (x + 0.01 * rng.standard_normal(t.size)).astype(np.float32)[None]
+
+
+def volumes_3d(batch: int, n: int, seed: int) -> np.ndarray:
+    """The 3-D configuration at side n (256 in the benchmark): spherical shells cos(2 pi r / 8), a plane
+    wave along z with its period rising from 32 to 64 voxels, a Gaussian trend of sigma 90 n / 256,
+    noise 0.01 N(0, 1); (batch, n, n, n) float32."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.mgrid[0:n, 0:n, 0:n].astype(np.float32)
+    out = np.empty((batch, n, n, n), np.float32)
+    period = 32 + 32 * z / (n - 1)
+    sigma = 90.0 * n / 256
+    for b in range(batch):
+        c = rng.uniform(0, n, 3)
+        r = np.sqrt((z - c[0]) ** 2 + (y - c[1]) ** 2 + (x - c[2]) ** 2)
+        g = rng.uniform(0, n, 3)
+        f = np.cos(2 * np.pi * r / 8) + np.cos(2 * np.pi * z / period)
+        f += 3 * np.exp(-((z - g[0]) ** 2 + (y - g[1]) ** 2 + (x - g[2]) ** 2) / (2 * sigma ** 2))
+        out[b] = f + 0.01 * rng.standard_normal((n, n, n)).astype(np.float32)
+    return out
+
+
+def signals_ragged(count: int, lo: int, hi: int, seed: int) -> list[np.ndarray]:
+    """The 1-D ragged configuration: lengths exp(U[ln lo, ln hi]); a linear chirp 0.002 -> 0.2
+    cycles/sample, 0.8 cos(w t + 0.8 sin w t) with w ~ U[0.05, 0.3], a slope ~ U[-1e-3, 1e-3], noise."""
+    rng = np.random.default_rng(seed)
+    xs = []
+    for _ in range(count):
+        n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        t = np.arange(n, dtype=np.float64)
+        w = rng.uniform(0.05, 0.3)
+        f = np.cos(2 * np.pi * (0.002 * t + 0.5 * (0.2 - 0.002) / n * t * t)) + 0.8 * np.cos(w * t + 0.8 * np.sin(w * t))
+        f += rng.uniform(-1e-3, 1e-3) * t + 0.01 * rng.standard_normal(n)
+        xs.append(f.astype(np.float32))
+    return xs
+
+
+def images_ragged(count: int, lo: int, hi: int, seed: int) -> list[np.ndarray]:
+    """The 2-D ragged configuration: height and width each U[lo, hi]; the 2-D recipe with the ring and
+    stripe periods and the blob width scaled by side / 512."""
+    rng = np.random.default_rng(seed)
+    xs = []
+    for _ in range(count):
+        h, w = (int(v) for v in rng.integers(lo, hi + 1, 2))
+        s = np.sqrt(h * w) / 512
+        y, x = np.mgrid[0:h, 0:w].astype(np.float32)
+        cy, cx = rng.uniform(0, h), rng.uniform(0, w)
+        f = np.cos(2 * np.pi * np.hypot(y - cy, x - cx) / (6 * s))
+        f += 1.5 * np.cos(2 * np.pi * (x + 4 * s * np.sin(2 * np.pi * y / (128 * s))) / (24 * s))
+        for _ in range(2):
+            by, bx = rng.uniform(0, h), rng.uniform(0, w)
+            f += 3 * np.exp(-((y - by) ** 2 + (x - bx) ** 2) / (2 * (80 * s) ** 2))
+        xs.append((f + 0.02 * rng.standard_normal((h, w))).astype(np.float32))
+    return xs
 
 
 def other_workload(name: str, seed: int):
     """The other configurations of the method's benchmark suite (seeded synthetic stand-ins):
     returns (description, list of fields or one batch array, axes, elements)."""
-    rng = np.random.default_rng(seed)
     if name == "1d":
-        t = np.arange(2048, dtype=np.float64)
-        x = np.sin(2 * np.pi * t / 8) + 2 * np.sin(2 * np.pi * t / 64) + 3 * np.sin(2 * np.pi * t / 512)
-        x = (x + 0.01 * rng.standard_normal(t.size)).astype(np.float32)[None]
-        return "1-D 1 x 2048 float32 (three tones and noise), sifts 3", x, (1,), 1
+        return "1-D 1 x 2048 float32 (three tones and noise), sifts 3", signal_1d(seed), (1,), 1
     if name == "3d":
-        n = 256
-        z, y, x = np.mgrid[0:n, 0:n, 0:n].astype(np.float32)
-        out = np.empty((4, n, n, n), np.float32)
-        period = 32 + 32 * z / (n - 1)
-        for b in range(4):
-            c = rng.uniform(0, n, 3)
-            r = np.sqrt((z - c[0]) ** 2 + (y - c[1]) ** 2 + (x - c[2]) ** 2)
-            g = rng.uniform(0, n, 3)
-            f = np.cos(2 * np.pi * r / 8) + np.cos(2 * np.pi * z / period)
-            f += 3 * np.exp(-((z - g[0]) ** 2 + (y - g[1]) ** 2 + (x - g[2]) ** 2) / (2 * 90.0 ** 2))
-            out[b] = f + 0.01 * rng.standard_normal((n, n, n)).astype(np.float32)
-        return "3-D 4 x 256^3 float32 (spherical waves, chirped plane wave, trend, noise), sifts 3", out, (1, 2, 3), 4
+        return ("3-D 4 x 256^3 float32 (spherical waves, chirped plane wave, trend, noise), sifts 3",
+                volumes_3d(4, 256, seed), (1, 2, 3), 4)
     if name == "ragged1d":
-        xs = []
-        for _ in range(1024):
-            n = int(np.exp(rng.uniform(np.log(256), np.log(8192))))
-            t = np.arange(n, dtype=np.float64)
-            w = rng.uniform(0.05, 0.3)
-            f = np.cos(2 * np.pi * (0.002 * t + 0.5 * (0.2 - 0.002) / n * t * t)) + 0.8 * np.cos(w * t + 0.8 * np.sin(w * t))
-            f += rng.uniform(-1e-3, 1e-3) * t + 0.01 * rng.standard_normal(n)
-            xs.append(f.astype(np.float32))
         return ("1-D ragged 1024 signals, lengths exp(U[ln 256, ln 8192]) float32 (chirp, FM tone, slope, noise), "
-                "sifts 3", xs, None, 1024)
+                "sifts 3", signals_ragged(1024, 256, 8192, seed), None, 1024)
     if name == "ragged2d":
-        xs = []
-        for _ in range(256):
-            h, w = (int(v) for v in rng.integers(64, 2049, 2))
-            s = np.sqrt(h * w) / 512
-            y, x = np.mgrid[0:h, 0:w].astype(np.float32)
-            cy, cx = rng.uniform(0, h), rng.uniform(0, w)
-            f = np.cos(2 * np.pi * np.hypot(y - cy, x - cx) / (6 * s))
-            f += 1.5 * np.cos(2 * np.pi * (x + 4 * s * np.sin(2 * np.pi * y / (128 * s))) / (24 * s))
-            for _ in range(2):
-                by, bx = rng.uniform(0, h), rng.uniform(0, w)
-                f += 3 * np.exp(-((y - by) ** 2 + (x - bx) ** 2) / (2 * (80 * s) ** 2))
-            xs.append((f + 0.02 * rng.standard_normal((h, w))).astype(np.float32))
         return ("2-D ragged 256 images, sides U[64, 2048] float32 (the 2-D recipe scaled by side / 512), sifts 3",
-                xs, None, 256)
+                images_ragged(256, 64, 2048, seed), None, 256)
     raise ValueError(name)
+
+
+def fp64_error(fields: list[np.ndarray], results: list[np.ndarray], threads: int) -> dict:
+    """The FP64 error of float32 results: each field is decomposed again by the oracle in float64
+    (the same sift, every rounding in double) and max |y - y64| over the rows is taken, rel = that
+    over max |x|; the worst element is reported. Elements whose float64 decisions (IMF count,
+    windows) differ from the float32 result's are counted apart (their rows are not comparable)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(i):
+        x = fields[i]
+        rows64, info64 = oracle.decompose(x[None].astype(np.float64))
+        y = np.asarray(results[i], dtype=np.float64)
+        k = int(info64["n_imfs"][0]) + 1
+        if y.shape[0] < k or np.any(y[k:] != 0):
+            return None
+        d = float(np.abs(y[:k] - rows64[0, :k]).max())
+        return d, d / float(np.abs(x).max())
+
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        out = list(ex.map(one, range(len(fields))))
+    ok = [o for o in out if o is not None]
+    return {"max_abs": max((o[0] for o in ok), default=None), "rel": max((o[1] for o in ok), default=None),
+            "n_checked": len(ok), "decisions_differ": len(out) - len(ok), "oracle": "float64 restatement of the sift"}
 
 
 def run_other(args) -> None:

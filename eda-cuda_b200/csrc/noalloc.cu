@@ -1,9 +1,14 @@
 // SPDX-License-Identifier: Apache-2.0
-// An allocation-free decomposition for callers that must not allocate device memory: code that runs
-// inside a CUDA stream capture or a graph it is building, plugin hosts whose allocator is not theirs
-// to call, or real-time loops that forbid allocation after start-up. It computes exactly what
-// eda_decompose computes (the same engine and kernels, bit for bit), for 1-D signals of bounded
-// size, with all of its scratch memory in the file-scope device array below.
+// An allocation-free decomposition for callers that must not allocate device memory: plugin hosts
+// whose device allocator belongs to the host application (an allocation behind its back breaks its
+// accounting or its memory limits), and real-time loops that forbid allocation after start-up (an
+// allocation can block on the driver for milliseconds). It computes exactly what eda_decompose
+// computes (the same engine and kernels, bit for bit), for 1-D signals of bounded size, with all of
+// its scratch memory in the file-scope device array below.
+//
+// The call is synchronous: the engine reads per-element state back to the host between the steps
+// of a mode and at the end of the call, so it blocks the host on the caller's stream several times
+// and cannot be recorded into a CUDA graph by stream capture.
 //
 // The array (kScratchBytes per device) is part of the library's image: every GPU that loads the
 // library holds it until the process exits. Every call shares it, and it keeps the last call's
@@ -45,6 +50,22 @@ void* scratch_address() {
     addr[dev] = p;
   }
   return addr[dev];
+}
+
+// A caller's buffer must be device memory of the current device (the scratch is that device's).
+void require_on_current_device(const void* ptr, const char* name) {
+  int dev = 0;
+  EDAB_CUDA(cudaGetDevice(&dev));
+  cudaPointerAttributes at{};
+  const cudaError_t e = cudaPointerGetAttributes(&at, ptr);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw std::invalid_argument(std::string("eda: eda_decompose_noalloc: ") + name + " is not a CUDA pointer");
+  }
+  if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != dev) {
+    throw std::invalid_argument(std::string("eda: eda_decompose_noalloc: ") + name + " must be device memory of the current device (" +
+                                std::to_string(dev) + ")");
+  }
 }
 
 size_t up256(size_t v) { return (v + 255) / 256 * 256; }
@@ -181,6 +202,8 @@ EDA_API int eda_decompose_noalloc(const void* x_dev, int dtype, int64_t batch, i
     p.max_chunk = 0;
     const int64_t n[1] = {length};
     edab::validate(dtype, 1, batch, n, p);
+    edab::require_on_current_device(x_dev, "x_dev");
+    edab::require_on_current_device(rows_dev, "rows_dev");
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (dtype == EDA_FLOAT32) {
       edab::run_noalloc<float>(static_cast<const float*>(x_dev), batch, length, p, static_cast<float*>(rows_dev),

@@ -176,20 +176,22 @@ EDA_API int eda_device_info(int device, char* buf, size_t len);
 EDA_API int eda_release_workspace(void);
 
 /* The allocation-free decomposition (no counterpart in the reference), for callers that must not
- * allocate device memory: code running inside a CUDA stream capture or a graph under construction,
- * plugin hosts that own the allocator, real-time loops that forbid allocation after start-up. It
- * computes what eda_decompose computes, bit for bit, for 1-D signals: x_dev holds batch x length
- * samples (C-contiguous, dtype 0 float32 / 1 float64) on the current device; rows_dev receives
- * (batch, rows_capacity, length) in the same layout as eda_run_collect with P = rows_capacity (NaN
- * rows for failed elements, zeros above an element's residue); *rows receives the P an
- * eda_decompose call would have (EDA_INVALID_ARGUMENT when it exceeds rows_capacity); the host
- * arrays n_imfs, error [batch] and windows, sifts, spacing, energy [batch, rows_capacity - 1] are
- * filled as eda_run_info fills them (NULL allowed). All scratch lives in a 24 MiB device array
+ * allocate device memory: plugin hosts whose device allocator belongs to the host application, and
+ * real-time loops that forbid allocation after start-up. It computes what eda_decompose computes,
+ * bit for bit, for 1-D signals: x_dev holds batch x length samples (C-contiguous, dtype 0 float32 /
+ * 1 float64) in device memory of the current device; rows_dev (device memory of the current device)
+ * receives (batch, rows_capacity, length) in the same layout as eda_run_collect with
+ * P = rows_capacity (NaN rows for failed elements, zeros above an element's residue); *rows receives
+ * the P an eda_decompose call would have (EDA_INVALID_ARGUMENT when it exceeds rows_capacity); the
+ * host arrays n_imfs, error [batch] and windows, sifts, spacing, energy [batch, rows_capacity - 1]
+ * are filled as eda_run_info fills them (NULL allowed). All scratch lives in a 24 MiB device array
  * inside the library, held by every GPU that loads the library until the process exits: batch x
  * length up to about 32768 float32 or 16384 float64 samples; larger calls are rejected with
- * EDA_INVALID_ARGUMENT. The first call on a device looks the array's address up (make it before any
- * stream capture). Calls share the array: calls that overlap on the GPU race, so serialize them.
- * It calls no cudaMalloc, cudaFree or allocating library routine. */
+ * EDA_INVALID_ARGUMENT, as are buffers that are not device memory of the current device. The first
+ * call on a device looks the array's address up. The call is synchronous: it blocks the host on the
+ * stream several times (per-element state is read back between the steps of a mode), so it cannot
+ * be recorded into a CUDA graph by stream capture. Calls share the array: calls that overlap on the
+ * GPU race, so serialize them. It calls no cudaMalloc, cudaFree or allocating library routine. */
 EDA_API int eda_decompose_noalloc(const void* x_dev, int dtype, int64_t batch, int64_t length,
                                   const eda_params* params, void* rows_dev, int32_t rows_capacity, int32_t* rows,
                                   int32_t* n_imfs, int32_t* error, int32_t* windows, int32_t* sifts, double* spacing,

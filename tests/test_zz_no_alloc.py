@@ -1,9 +1,10 @@
 # SPDX-License-Identifier: Apache-2.0
 """The allocation-free decomposition (eda_decompose_noalloc) through the C ABI: for callers that
-cannot allocate device memory (inside a stream capture, in plugin hosts that own the allocator,
-in loops that forbid allocation after start-up), it must return what eda_decompose returns, bit
-for bit (the tolerance of the 1-D parity tests), on consecutive calls that share its scratch, and
-reject a call larger than its scratch with a clear error. The test allocates the input and output
+cannot allocate device memory (plugin hosts whose allocator belongs to the host application, loops
+that forbid allocation after start-up), it must return what eda_decompose returns, bit for bit
+(the tolerance of the 1-D parity tests), on consecutive calls that share its scratch, take no
+device memory on a warm call, and reject a call larger than its scratch or buffers that are not
+device memory of the current device with a clear error. The test allocates the input and output
 buffers itself; the entry point allocates nothing.
 
 This file is collected last (tests/test_zz_*), so a run that stops at its first failure has run
@@ -71,6 +72,9 @@ def parts():
         pytest.skip("no CUDA device")
     core = _native.core()
     lib = core._lib
+    vp, i32p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)
+    lib.eda_decompose_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, vp, vp, ctypes.c_int32,
+                                          i32p, vp, vp, vp, vp, vp, vp, vp]
     lib.eda_decompose_noalloc.restype = ctypes.c_int
     return torch, core, lib
 
@@ -106,3 +110,49 @@ def test_noalloc_rejects_a_call_beyond_its_scratch(parts):
     want_rows, _ = core.decompose_host(x, -1, None, 3, True, False, 0)
     st, P, (rows, _) = _noalloc(lib, core, x, 16, torch)
     assert st == 0 and np.array_equal(rows[:, :P], want_rows)
+
+
+def test_noalloc_takes_no_device_memory(parts):
+    """A warm call leaves the device's free memory unchanged (nothing allocated, nothing freed: no
+    workspace, no pool, no library allocation); the buffers are made before the measurement."""
+    torch, core, lib = parts
+    from eda._native import _Params
+
+    x = _signals(4, 2048, 21).astype(np.float32)
+    B, n = x.shape
+    dev = torch.device("cuda", 0)
+    x_dev = torch.from_numpy(x).to(dev)
+    rows_dev = torch.zeros((B, 16, n), dtype=torch.float32, device=dev)
+    P = ctypes.c_int32(0)
+    params = _Params(-1, -1.0, 3, 1, 0)
+    stream = torch.cuda.current_stream(dev)
+
+    def call():
+        st = lib.eda_decompose_noalloc(ctypes.c_void_p(x_dev.data_ptr()), 0, B, n, ctypes.byref(params),
+                                       ctypes.c_void_p(rows_dev.data_ptr()), 16, ctypes.byref(P),
+                                       None, None, None, None, None, None, ctypes.c_void_p(stream.cuda_stream))
+        torch.cuda.synchronize(dev)
+        return st
+
+    assert call() == 0  # warm: the kernels of the path are loaded
+    free0, _ = torch.cuda.mem_get_info(dev)
+    assert call() == 0
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+
+
+def test_noalloc_rejects_host_buffers(parts):
+    torch, core, lib = parts
+    from eda._native import _Params
+
+    x = _signals(2, 512, 5).astype(np.float32)
+    rows = np.zeros((2, 16, 512), np.float32)
+    P = ctypes.c_int32(0)
+    params = _Params(-1, -1.0, 3, 1, 0)
+    st = lib.eda_decompose_noalloc(ctypes.c_void_p(x.ctypes.data), 0, 2, 512, ctypes.byref(params),
+                                   ctypes.c_void_p(rows.ctypes.data), 16, ctypes.byref(P),
+                                   None, None, None, None, None, None, None)
+    assert st == 1
+    buf = ctypes.create_string_buffer(1024)
+    lib.eda_last_error(buf, len(buf))
+    assert "device memory" in buf.value.decode()
