@@ -44,6 +44,9 @@ void cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 // Every kernel launch of the engine is followed by EDAB_LAUNCH: it checks the launch and counts it
 // for the instrumentation (profile.cu).
 void note_launch();
+// True on the first call for `key` (a kernel) on the current device, false after: kernel
+// attributes such as the dynamic shared-memory limit are set per device. Thread-safe.
+bool first_on_device(const void* key);
 #define EDAB_LAUNCH(name)            \
   do {                               \
     ::edab::note_launch();           \

@@ -217,25 +217,24 @@ __device__ __forceinline__ void element_de(T L, T c, T q, T span_m1, T* d, T* e)
   *e = mul_rn(T(0.5), diff > T(0) ? diff : T(0));
 }
 
-// Element build: o = e n, the per-element min / max of d (CTA reduction, one atomic per CTA).
+// The element's extent (cpp/src/method/element.cu:182-226): per voxel d and e, the segment
+// offset o = e n (D >= 2), and the element's smallest and largest d (as double bits: d >= 0).
+// The voxel keeps d in the weight field t and whether its segment reaches past a quarter sample
+// (e > 1/4, the rungs that need segment points) in the rung field lo, so the rung pass that
+// follows reads 5 bytes per voxel instead of recomputing d and e from L and c. Extremes: a warp
+// folds its lanes' by shuffles, one atomic per warp.
 template <class T, int D>
-__global__ void __launch_bounds__(kThreads) build_kernel(Geom g, Ctl c, const T* __restrict__ L,
-                                                        const T* __restrict__ coh, const T* n0, const T* n1,
-                                                        const T* n2, T* o0, T* o1, T* o2, Elem* el,
-                                                        const int32_t* run) {
-  __shared__ unsigned long long smin, smax;
+__global__ void __launch_bounds__(kThreads) element_extent(Geom g, Ctl c, const T* __restrict__ L,
+                                                          const T* __restrict__ coh, const T* n0, const T* n1,
+                                                          const T* n2, T* o0, T* o1, T* o2, T* d_out,
+                                                          uint8_t* far_out, Elem* el, const int32_t* run) {
   const int64_t b = blockIdx.y;
   if (!run[b]) return;
-  if (threadIdx.x == 0) {
-    smin = 0x7ff0000000000000ULL;
-    smax = 0ULL;
-  }
-  __syncthreads();
   const T q = static_cast<T>(c.q), sm1 = static_cast<T>(c.span - 1.0);
-  unsigned long long tmin = 0x7ff0000000000000ULL, tmax = 0ULL;
+  uint64_t lo_bits = ~0ULL, hi_bits = 0ULL;
   const int32_t nl = g.n_last;
-  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
-       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field; v += step) {
     if (pitch_col(g, v) >= nl) continue;
     const int64_t i = b * g.field + v;
     T d, e;
@@ -245,80 +244,71 @@ __global__ void __launch_bounds__(kThreads) build_kernel(Geom g, Ctl c, const T*
       o1[i] = mul_rn(e, n1[i]);
       if constexpr (D == 3) o2[i] = mul_rn(e, n2[i]);
     }
-    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(d)));
-    tmin = bits < tmin ? bits : tmin;
-    tmax = bits > tmax ? bits : tmax;
+    d_out[i] = d;
+    far_out[i] = e > T(0.25) ? 1 : 0;
+    const uint64_t bits = static_cast<uint64_t>(__double_as_longlong(static_cast<double>(d)));
+    lo_bits = bits < lo_bits ? bits : lo_bits;
+    hi_bits = bits > hi_bits ? bits : hi_bits;
   }
-  atomicMin(&smin, tmin);
-  atomicMax(&smax, tmax);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    atomicMin(reinterpret_cast<unsigned long long*>(&el[b].d_min_bits), smin);
-    atomicMax(reinterpret_cast<unsigned long long*>(&el[b].d_max_bits), smax);
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) {
+    const uint64_t a = __shfl_xor_sync(0xffffffffu, lo_bits, m), z = __shfl_xor_sync(0xffffffffu, hi_bits, m);
+    lo_bits = a < lo_bits ? a : lo_bits;
+    hi_bits = z > hi_bits ? z : hi_bits;
+  }
+  if ((threadIdx.x & 31) == 0 && hi_bits >= lo_bits) {  // the warp saw a voxel
+    atomicMin(reinterpret_cast<unsigned long long*>(&el[b].d_min_bits), static_cast<unsigned long long>(lo_bits));
+    atomicMax(reinterpret_cast<unsigned long long*>(&el[b].d_max_bits), static_cast<unsigned long long>(hi_bits));
   }
 }
 
-// The hat weights in log d (cpp/src/method/element.cu:228-292): lo, t and the rung flags.
-template <class T, int D>
-__global__ void __launch_bounds__(kThreads) weights_kernel(Geom g, Ctl c, const T* __restrict__ L,
-                                                          const T* __restrict__ coh, Elem* el, uint8_t* lo, T* t,
-                                                          const int32_t* run) {
-  __shared__ double slw[kMaxRungs];
-  __shared__ unsigned s_used, s_pts;
+// The voxel's place on the element's ladder (cpp/src/method/element.cu:228-292): with the ladder's
+// logs lw_0 < .. < lw_{K-1}, the bracket j of log(clamp(d, w_0, w_{K-1})) (the last rung whose log
+// is at most it, kept inside 0 .. K - 2, found by bisection) and the hat weight t of rung j + 1
+// (rung j weighs 1 - t). The rung masks: rungs some voxel weighs (used) and those of voxels whose
+// segment reaches past a quarter sample (pts); a warp ORs its lanes', one atomic per warp. Reads d
+// from t and the reach bit from lo (element_extent), then overwrites both.
+template <class T>
+__global__ void __launch_bounds__(kThreads) element_rungs(Geom g, uint8_t* lo, T* t, Elem* el, const int32_t* run) {
+  __shared__ double lw[kMaxRungs];
   const int64_t b = blockIdx.y;
   if (!run[b]) return;
   const int K = el[b].n_rungs;
-  if (threadIdx.x < kMaxRungs) slw[threadIdx.x] = threadIdx.x < static_cast<unsigned>(K) ? el[b].rung_lw[threadIdx.x] : 0.0;
-  if (threadIdx.x == 0) {
-    s_used = 0u;
-    s_pts = 0u;
-  }
+  if (threadIdx.x < kMaxRungs) lw[threadIdx.x] = static_cast<int>(threadIdx.x) < K ? el[b].rung_lw[threadIdx.x] : 0.0;
   __syncthreads();
-  const T q = static_cast<T>(c.q), sm1 = static_cast<T>(c.span - 1.0);
-  const double w_lo = static_cast<double>(el[b].rung_w[0]);
-  const double w_hi = static_cast<double>(el[b].rung_w[K > 0 ? K - 1 : 0]);
+  const double w_first = static_cast<double>(el[b].rung_w[0]);
+  const double w_last = static_cast<double>(el[b].rung_w[K > 0 ? K - 1 : 0]);
   unsigned used = 0u, pts = 0u;
   const int32_t nl = g.n_last;
-  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
-       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field; v += step) {
     if (pitch_col(g, v) >= nl) continue;
     const int64_t i = b * g.field + v;
-    T d, e;
-    element_de<T>(L[i], D == 1 ? T(0) : coh[i], q, sm1, &d, &e);
-    int idx = 0;
-    T tt = T(0);
+    const bool far = lo[i] != 0;
+    int j = 0;
+    T w = T(0);
     if (K > 1) {
-      double dc = static_cast<double>(d);
-      dc = dc > w_lo ? dc : w_lo;
-      dc = dc < w_hi ? dc : w_hi;
-      const double lg = log(dc);
-      int cnt = 0;
-      for (int j = 0; j < K; ++j) cnt += slw[j] <= lg ? 1 : 0;
-      idx = cnt - 1;
-      idx = idx < 0 ? 0 : (idx > K - 2 ? K - 2 : idx);
-      tt = static_cast<T>(__ddiv_rn(__dsub_rn(lg, slw[idx]), __dsub_rn(slw[idx + 1], slw[idx])));
+      const double x = log(fmin(fmax(static_cast<double>(t[i]), w_first), w_last));
+      int lo_j = 0, hi_j = K;  // lw[lo_j - 1] <= x < lw[hi_j]
+      while (lo_j < hi_j) {
+        const int mid = (lo_j + hi_j) >> 1;
+        if (lw[mid] <= x) lo_j = mid + 1;
+        else hi_j = mid;
+      }
+      j = min(max(lo_j - 1, 0), K - 2);
+      w = static_cast<T>(__ddiv_rn(__dsub_rn(x, lw[j]), __dsub_rn(lw[j + 1], lw[j])));
     }
-    lo[i] = static_cast<uint8_t>(idx);
-    t[i] = tt;
-    const T wl = sub_rn(T(1), tt);
-    unsigned bits = 0u;
-    if (wl > T(0)) bits |= 1u << idx;
-    if (tt > T(0)) bits |= 1u << (idx + 1);
-    used |= bits;
-    if (e > T(0.25)) pts |= bits;
+    lo[i] = static_cast<uint8_t>(j);
+    t[i] = w;
+    const unsigned mine = (sub_rn(T(1), w) > T(0) ? 1u << j : 0u) | (w > T(0) ? 1u << (j + 1) : 0u);
+    used |= mine;
+    if (far) pts |= mine;
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    used |= __shfl_xor_sync(0xffffffffu, used, off);
-    pts |= __shfl_xor_sync(0xffffffffu, pts, off);
-  }
+  used = __reduce_or_sync(0xffffffffu, used);
+  pts = __reduce_or_sync(0xffffffffu, pts);
   if ((threadIdx.x & 31) == 0) {
-    if (used) atomicOr(&s_used, used);
-    if (pts) atomicOr(&s_pts, pts);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (s_used) atomicOr(&el[b].rung_used, s_used);
-    if (s_pts) atomicOr(&el[b].rung_pts, s_pts);
+    if (used) atomicOr(&el[b].rung_used, used);
+    if (pts) atomicOr(&el[b].rung_pts, pts);
   }
 }
 
@@ -1033,11 +1023,11 @@ void Engine<T>::orientation_and_build() {
   }
   const dim3 grid = voxel_grid(g_);
   switch (g_.dim) {
-    case 1: build_kernel<T, 1><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, el_, on); break;
-    case 2: build_kernel<T, 2><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, n_[0], n_[1], nullptr, o_[0], o_[1], nullptr, el_, on); break;
-    default: build_kernel<T, 3><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, n_[0], n_[1], n_[2], o_[0], o_[1], o_[2], el_, on); break;
+    case 1: element_extent<T, 1><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, t_, lo_, el_, on); break;
+    case 2: element_extent<T, 2><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, n_[0], n_[1], nullptr, o_[0], o_[1], nullptr, t_, lo_, el_, on); break;
+    default: element_extent<T, 3><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, n_[0], n_[1], n_[2], o_[0], o_[1], o_[2], t_, lo_, el_, on); break;
   }
-  EDAB_LAUNCH("build_kernel");
+  EDAB_LAUNCH("element_extent");
 }
 
 // return_orientation: n with the canonical sign (the first component of magnitude above the dtype's
@@ -1103,13 +1093,8 @@ bool Engine<T>::ladder_and_weights(int32_t* n_rungs_max) {
     const int j = static_cast<int>(i % kMaxRungs);
     if (on[b] && j < el[b].n_rungs) el[b].rung_lw[j] = log(static_cast<double>(el[b].rung_w[j]));
   });
-  const dim3 grid = voxel_grid(g_);
-  switch (g_.dim) {
-    case 1: weights_kernel<T, 1><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, el_, lo_, t_, on); break;
-    case 2: weights_kernel<T, 2><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, el_, lo_, t_, on); break;
-    default: weights_kernel<T, 3><<<grid, kThreads, 0, s_>>>(g_, c_, L_, coh_, el_, lo_, t_, on); break;
-  }
-  EDAB_LAUNCH("weights_kernel");
+  element_rungs<T><<<voxel_grid(g_), kThreads, 0, s_>>>(g_, lo_, t_, el_, on);
+  EDAB_LAUNCH("element_rungs");
   int32_t* rw = rung_win_;
   const int64_t B = B_;
   for_samples(s_, B_ * kMaxRungs, [=] __device__(int64_t i) {

@@ -215,41 +215,127 @@ __device__ __forceinline__ double dct_freq(const Geom& g, const int32_t* k, doub
   return __dsqrt_rn(r2);
 }
 
-// The Jacobi rotation of the reference's eigen pass (Rutishauser's stable form).
-__device__ __forceinline__ void jacobi_rotate(double (&A)[3][3], double (&V)[3][3], int p, int q, int r, int dim) {
-  const double apq = A[p][q];
-  if (apq == 0.0) return;
-  const double theta = __ddiv_rn(__dsub_rn(A[q][q], A[p][p]), __dmul_rn(2.0, apq));
-  const double at = fabs(theta);
-  const double t = __ddiv_rn(copysign(1.0, theta), __dadd_rn(at, __dsqrt_rn(__dadd_rn(__dmul_rn(theta, theta), 1.0))));
-  const double c = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(__dmul_rn(t, t), 1.0)));
-  const double s = __dmul_rn(t, c);
-  const double tau = __ddiv_rn(s, __dadd_rn(1.0, c));
-  const double tapq = __dmul_rn(t, apq);
-  A[p][p] = __dsub_rn(A[p][p], tapq);
-  A[q][q] = __dadd_rn(A[q][q], tapq);
-  A[p][q] = A[q][p] = 0.0;
-  if (r >= 0) {
-    const double gg = A[r][p], hh = A[r][q];
-    const double np_ = __dsub_rn(gg, __dmul_rn(s, __dadd_rn(hh, __dmul_rn(gg, tau))));
-    const double nq_ = __dadd_rn(hh, __dmul_rn(s, __dsub_rn(gg, __dmul_rn(hh, tau))));
-    A[r][p] = A[p][r] = np_;
-    A[r][q] = A[q][r] = nq_;
-  }
-  for (int k = 0; k < dim; ++k) {
-    const double gg = V[k][p], hh = V[k][q];
-    V[k][p] = __dsub_rn(gg, __dmul_rn(s, __dadd_rn(hh, __dmul_rn(gg, tau))));
-    V[k][q] = __dadd_rn(hh, __dmul_rn(s, __dsub_rn(gg, __dmul_rn(hh, tau))));
-  }
-}
-
 template <int D>
 __host__ __device__ constexpr int tensor_pair(int a, int b) {
   return D == 2 ? (a == 0 ? b : 2) : (a == 0 ? b : (a == 1 ? 2 + b : 5));
 }
 
-// T = R1 R1^T + R2 R2^T in T, then the eigen pass in double: n the top eigenvector, c = (mu1 -
-// mu2) / (mu1 + mu2) clipped to [0, 1].
+// ---------------------------------------------------------------------------------------------
+// The eigen step of the orientation: the top eigenvector n and the coherence c = (mu1 - mu2) /
+// (mu1 + mu2) (clipped to [0, 1]) of the symmetric D x D energy tensor of every voxel
+// (cpp/src/method/element.cu:49-164 computes the same quantities).
+//
+// Cyclic Jacobi with half-angle rotations: for a pair (p, q) with off-diagonal value b and half
+// difference h = (A_qq - A_pp) / 2, r = hypot(h, b), the rotation J (cos t, sin t) with
+// cos 2t = |h| / r that zeroes A_pq is applied as A <- J^T A J and V <- V J. A 2 x 2 tensor is
+// diagonal after one rotation; a 3 x 3 one after a few sweeps (quadratic convergence), on the
+// tensor prescaled by a power of two (exact) so that no product leaves the range.
+//
+// Precision: float32 fields solve in float (4 sweeps); where the gap (mu1 - mu2) / (mu1 + mu2) falls
+// below kEigenGap the direction is ill-conditioned in float (its error grows as eps / gap) and the
+// voxel is solved again in double (6 sweeps) from the same tensor. Float64 fields always solve in
+// double. The direction's sign: its largest component (the first on a tie) is positive.
+constexpr double kEigenGap = 1e-2;
+
+template <class S, int D>
+__device__ __forceinline__ void jacobi_pair(S (&A)[3][3], S (&V)[3][3], int p, int q) {
+  const S b = A[p][q];
+  if (b == S(0)) return;
+  const S h = (A[q][q] - A[p][p]) * S(0.5);
+  const S r = hypot(h, b);
+  // cos t and sin t of the smaller rotation angle t (|t| <= pi / 4): tan 2t = b / h
+  const S c = sqrt((S(1) + fabs(h) / r) * S(0.5));
+  const S sn = (h < S(0) ? S(-1) : S(1)) * b / (S(2) * r * c);
+  // columns p and q of A J, then rows p and q of J^T (A J)
+  S AJ[3][3];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+#pragma unroll
+    for (int j = 0; j < D; ++j) AJ[i][j] = A[i][j];
+    AJ[i][p] = c * A[i][p] - sn * A[i][q];
+    AJ[i][q] = sn * A[i][p] + c * A[i][q];
+  }
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    const S up = c * AJ[p][j] - sn * AJ[q][j];
+    const S uq = sn * AJ[p][j] + c * AJ[q][j];
+#pragma unroll
+    for (int i = 0; i < D; ++i) A[i][j] = AJ[i][j];
+    A[p][j] = up;
+    A[q][j] = uq;
+  }
+  A[p][q] = A[q][p] = S(0);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    const S vp = V[i][p], vq = V[i][q];
+    V[i][p] = c * vp - sn * vq;
+    V[i][q] = sn * vp + c * vq;
+  }
+}
+
+// The eigen decomposition of the tensor A0 (double copies of the T entries) in precision S: the
+// top eigenvector into nv, the coherence into *coh; returns the gap (mu1 - mu2) / (mu1 + mu2).
+template <class S, int D>
+__device__ __forceinline__ double eigen_top(const double (&A0)[3][3], double* nv, double* coh) {
+  S A[3][3], V[3][3];
+  double amax = 0.0;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) amax = fmax(amax, fabs(A0[i][j]));
+  const double scale = (amax > 0.0 && amax < d_inf()) ? scalbn(1.0, -ilogb(amax)) : 1.0;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      A[i][j] = static_cast<S>(A0[i][j] * scale);
+      V[i][j] = i == j ? S(1) : S(0);
+    }
+  if constexpr (D == 2) {
+    jacobi_pair<S, 2>(A, V, 0, 1);
+  } else {
+    constexpr int kSweeps = sizeof(S) == 4 ? 4 : 6;
+#pragma unroll 1
+    for (int sweep = 0; sweep < kSweeps; ++sweep) {
+      jacobi_pair<S, 3>(A, V, 0, 1);
+      jacobi_pair<S, 3>(A, V, 0, 2);
+      jacobi_pair<S, 3>(A, V, 1, 2);
+    }
+  }
+  // the top eigenvalue (the first on a tie), the largest of the others, the top column of V; by
+  // selects over compile-time indices (a run-time index would put A and V in local memory)
+  int top = 0;
+  S mu1 = A[0][0];
+#pragma unroll
+  for (int a = 1; a < D; ++a) {
+    if (A[a][a] > mu1) {
+      mu1 = A[a][a];
+      top = a;
+    }
+  }
+  S mu2 = -inf_t<S>();
+  S col[3] = {S(0), S(0), S(0)};
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    if (a != top && A[a][a] > mu2) mu2 = A[a][a];
+#pragma unroll
+    for (int j = 0; j < D; ++j) col[a] = j == top ? V[a][j] : col[a];
+  }
+  S lead = col[0];
+#pragma unroll
+  for (int a = 1; a < D; ++a) lead = fabs(col[a]) > fabs(lead) ? col[a] : lead;
+  const S sgn = lead < S(0) ? S(-1) : S(1);
+#pragma unroll
+  for (int a = 0; a < D; ++a) nv[a] = static_cast<double>(sgn * col[a]);
+  const S sum = mu1 + mu2;
+  S cv = sum > S(0) ? (mu1 - mu2) / sum : S(0);
+  cv = cv < S(0) ? S(0) : (cv > S(1) ? S(1) : cv);
+  *coh = static_cast<double>(cv);
+  return static_cast<double>(cv);
+}
+
+// The energy tensor T = R1 R1^T + R2 R2^T of every voxel in the field's dtype (the reference's
+// rounding order: R1_a R1_c, then + R2_ak R2_kc for k = 0 .. D - 1), then its eigen step.
 template <class T, int D>
 __global__ void __launch_bounds__(256) tensor_eigen(Geom g, const int32_t* run, const T* __restrict__ work_r1,
                                                     const T* __restrict__ work_r2, T* n0, T* n1, T* n2, T* coh,
@@ -259,6 +345,7 @@ __global__ void __launch_bounds__(256) tensor_eigen(Geom g, const int32_t* run, 
   const int32_t nl = g.n[D - 1];
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     if (!run[b]) continue;
+    bool bad = false;
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       if (pitch_col(g, v) >= nl) continue;
@@ -269,73 +356,33 @@ __global__ void __launch_bounds__(256) tensor_eigen(Geom g, const int32_t* run, 
 #pragma unroll
       for (int p = 0; p < K; ++p) R2[p] = work_r2[p * F + i];
       double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
       bool finite = true;
 #pragma unroll
       for (int a = 0; a < D; ++a) {
 #pragma unroll
         for (int c = a; c < D; ++c) {
-          T vv = mul_rn(R1[a], R1[c]);
+          T acc = mul_rn(R1[a], R1[c]);
 #pragma unroll
           for (int k = 0; k < D; ++k) {
-            const T hak = R2[tensor_pair<D>(a < k ? a : k, a < k ? k : a)];
-            const T hkc = R2[tensor_pair<D>(k < c ? k : c, k < c ? c : k)];
-            vv = add_rn(vv, mul_rn(hak, hkc));
+            acc = add_rn(acc, mul_rn(R2[tensor_pair<D>(min(a, k), max(a, k))], R2[tensor_pair<D>(min(k, c), max(k, c))]));
           }
-          const double dv = static_cast<double>(vv);
-          finite = finite && isfinite(dv);
-          A[a][c] = A[c][a] = dv;
+          A[a][c] = A[c][a] = static_cast<double>(acc);
+          finite = finite && isfinite(A[a][c]);
         }
       }
-      if (!finite) el[b].nonfinite = 1;
-      if constexpr (D == 2) {
-        jacobi_rotate(A, V, 0, 1, -1, 2);
+      bad = bad || !finite;
+      double nv[3] = {0, 0, 0}, cv = 0.0;
+      if constexpr (std::is_same_v<T, float>) {
+        if (eigen_top<float, D>(A, nv, &cv) < kEigenGap) eigen_top<double, D>(A, nv, &cv);
       } else {
-        double amax = 0.0;
-        for (int a = 0; a < 3; ++a)
-          for (int c = a; c < 3; ++c) amax = fmax(amax, fabs(A[a][c]));
-        if (amax > 0.0 && amax < INFINITY) {
-          const double sc = scalbn(1.0, -ilogb(amax));
-          for (int a = 0; a < 3; ++a)
-            for (int c = 0; c < 3; ++c) A[a][c] = __dmul_rn(A[a][c], sc);
-        }
-#pragma unroll 1
-        for (int sweep = 0; sweep < 6; ++sweep) {
-          jacobi_rotate(A, V, 0, 1, 2, 3);
-          jacobi_rotate(A, V, 0, 2, 1, 3);
-          jacobi_rotate(A, V, 1, 2, 0, 3);
-        }
+        eigen_top<double, D>(A, nv, &cv);
       }
-      double mu[D];
-#pragma unroll
-      for (int a = 0; a < D; ++a) mu[a] = A[a][a];
-      int top = 0;
-#pragma unroll
-      for (int a = 1; a < D; ++a) top = mu[a] > mu[top] ? a : top;
-      double mu2 = -INFINITY;
-#pragma unroll
-      for (int a = 0; a < D; ++a) mu2 = (a != top && mu[a] > mu2) ? mu[a] : mu2;
-      double mu1 = mu[0];
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        if (a == top) mu1 = mu[a];
-      }
-      double nv[D];
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        double vv = V[a][0];
-#pragma unroll
-        for (int c = 1; c < D; ++c) vv = c == top ? V[a][c] : vv;
-        nv[a] = vv;
-      }
-      const double ssum = __dadd_rn(mu1, mu2);
-      double cv = ssum > 0.0 ? __ddiv_rn(__dsub_rn(mu1, mu2), ssum) : 0.0;
-      cv = cv < 0.0 ? 0.0 : (cv > 1.0 ? 1.0 : cv);
       coh[i] = static_cast<T>(cv);
       n0[i] = static_cast<T>(nv[0]);
       n1[i] = static_cast<T>(nv[1]);
       if constexpr (D == 3) n2[i] = static_cast<T>(nv[2]);
     }
+    if (bad) el[b].nonfinite = 1;
   }
 }
 

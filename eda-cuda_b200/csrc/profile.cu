@@ -7,6 +7,8 @@
 
 #include <atomic>
 #include <mutex>
+#include <set>
+#include <utility>
 #include <vector>
 
 namespace edab {
@@ -24,6 +26,15 @@ __device__ unsigned long long g_cube_bytes;
 }  // namespace
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+bool first_on_device(const void* key) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> seen;
+  int dev = 0;
+  EDAB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  return seen.emplace(dev, key).second;
+}
 
 bool profiling() { return g_on.load(std::memory_order_relaxed); }
 

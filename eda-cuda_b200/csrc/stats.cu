@@ -7,6 +7,8 @@
 // of atomics or on the launch shape.
 #include "engine.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 
@@ -155,29 +157,39 @@ __global__ void __launch_bounds__(kThreads) element_totals(Geom g, const RowPart
 }
 
 // ---------------------------------------------------------------------------------------------
-// Selections: MSD radix select over the 64-bit order keys of the values (as doubles), 11-bit
-// digits (six passes: 11 x 5 + 9), two ranks at once (a median's middle pair, a quantile's
-// neighbours). Histograms: shared-memory u32 bins flushed into u64 global bins.
-constexpr int kSelBits = 11;
-constexpr int kSelBins = 1 << kSelBits;
-constexpr int kSelPasses = 6;
+// Exact selections (order statistics) by most-significant-digit radix selection on order keys,
+// unsigned integers that sort as the values do (-0 counts as +0). Float32 items without a centre
+// select on 32-bit keys of the float values (three digits: 11, 11 and 10 bits); every other
+// selection on 64-bit keys of the values as doubles (six digits: five of 11 bits, one of 9).
+//
+// One thread-block cluster (up to 8 CTAs) serves one element, all digits in one launch: each CTA
+// counts its share of the items per digit value in shared memory; the counts are added into the
+// cluster leader's shared table through distributed shared memory; the leader's threads find the
+// digit value that holds the wanted rank by a block-wide prefix sum and publish the extended prefix.
+// Two ranks are followed at once (a median's middle pair, a quantile's neighbours); they share one
+// table while their resolved digits agree.
+namespace cg = cooperative_groups;
 
-struct alignas(16) SelState {
-  uint64_t prefix[2];
-  uint64_t rank[2];
-  int64_t count;
-  double gamma;
-  int32_t valid, same;
-};
+constexpr int kDigitBits = 11;
+constexpr int kDigitBins = 1 << kDigitBits;
+constexpr int kSelClusterMax = 8;
+constexpr size_t kSelSmem = 2 * kDigitBins * sizeof(unsigned long long) + 2 * kDigitBins * sizeof(uint32_t);
 
-__device__ __forceinline__ uint64_t sel_key(double d) {
-  uint64_t u = static_cast<uint64_t>(__double_as_longlong(d));
-  if ((u << 1) == 0) u = 0;
-  return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+__device__ __forceinline__ uint32_t order_key(float v) {
+  uint32_t u = __float_as_uint(v);
+  if ((u & 0x7fffffffu) == 0u) u = 0u;
+  return (u & 0x80000000u) ? ~u : (u ^ 0x80000000u);
 }
-__device__ __forceinline__ double sel_value(uint64_t k) {
-  const uint64_t u = (k >> 63) ? (k & 0x7fffffffffffffffULL) : ~k;
-  return bits_d(u);
+__device__ __forceinline__ uint64_t order_key(double v) {
+  uint64_t u = static_cast<uint64_t>(__double_as_longlong(v));
+  if ((u & 0x7fffffffffffffffULL) == 0ULL) u = 0ULL;
+  return (u >> 63) ? ~u : (u ^ 0x8000000000000000ULL);
+}
+__device__ __forceinline__ double key_value(uint32_t k) {
+  return static_cast<double>(__uint_as_float((k & 0x80000000u) ? (k ^ 0x80000000u) : ~k));
+}
+__device__ __forceinline__ double key_value(uint64_t k) {
+  return bits_d((k >> 63) ? (k ^ 0x8000000000000000ULL) : ~k);
 }
 
 template <class T>
@@ -188,204 +200,219 @@ struct SelView {
   int64_t items;
 };
 
+// Item t of element b (a voxel, or a forward difference along one of the pooled axes) as a value of
+// the element's dtype; false where t is a pad, masked out, or has no forward neighbour.
 template <class T>
-__device__ __forceinline__ bool sel_item(const Geom& g, const SelView<T>& a, int64_t b, int64_t t, double* out) {
-  double val;
+__device__ __forceinline__ bool sel_raw(const Geom& g, const SelView<T>& a, int64_t b, int64_t t, T* out) {
   if (a.sel.src == SelSrc::kField) {
     if (is_pad(g, t)) return false;
     const int64_t i = b * g.field + t;
     if (a.sel.mask != nullptr && (a.sel.mask[i] & a.sel.bits) == 0) return false;
-    val = static_cast<double>(a.sel.field[i]);
-  } else {
-#ifdef __CUDA_ARCH__
-    const int64_t k = static_cast<int64_t>(__umul64hi(static_cast<uint64_t>(t), g.field_inv));  // t < 3 field
-#else
-    const int64_t k = t / g.field;
-#endif
-    const int64_t v = t - k * g.field;
-    const int axis = k == 0 ? a.ax[0] : (k == 1 ? a.ax[1] : a.ax[2]);
-    if (is_pad(g, v) || coord_of(g, v, axis) >= geom_n(g, axis) - 1) return false;
-    const int64_t i = b * g.field + v;
-    const int64_t st = axis == g.dim - 1 ? 1 : geom_stride(g, axis);
-    val = static_cast<double>(sub_rn(a.sel.field[i + st], a.sel.field[i]));
+    *out = a.sel.field[i];
+    return true;
   }
-  if (a.sel.center != nullptr) val = fabs(__dsub_rn(val, a.sel.center[b]));
-  *out = val;
+  const int64_t k = static_cast<int64_t>(__umul64hi(static_cast<uint64_t>(t), g.field_inv));  // t < 3 field
+  const int64_t v = t - k * g.field;
+  const int axis = k == 0 ? a.ax[0] : (k == 1 ? a.ax[1] : a.ax[2]);
+  if (is_pad(g, v) || coord_of(g, v, axis) >= geom_n(g, axis) - 1) return false;
+  const int64_t i = b * g.field + v;
+  const int64_t st = axis == g.dim - 1 ? 1 : geom_stride(g, axis);
+  *out = sub_rn(a.sel.field[i + st], a.sel.field[i]);
+  return true;
+}
+template <class T, class K>
+__device__ __forceinline__ bool sel_key_of(const Geom& g, const SelView<T>& a, int64_t b, int64_t t, K* key) {
+  T v;
+  if (!sel_raw(g, a, b, t, &v)) return false;
+  if constexpr (sizeof(K) == 4) {
+    *key = order_key(static_cast<float>(v));
+  } else {
+    double d = static_cast<double>(v);
+    if (a.sel.center != nullptr) d = fabs(__dsub_rn(d, a.sel.center[b]));
+    *key = order_key(d);
+  }
   return true;
 }
 
-template <class T>
-__global__ void __launch_bounds__(kThreads) sel_hist(Geom g, SelView<T> a, const int32_t* run, SelState* st,
-                                                     uint64_t* hist, int32_t nblk, int32_t shift, int32_t width,
-                                                     int32_t first) {
-  __shared__ uint32_t h[2][kSelBins];
-  const int64_t b = blockIdx.y;
-  if (run && !run[b]) return;
-  const SelState S = st[b];
-  if (!first && !S.valid) return;
-  const int nr = (first || S.same) ? 1 : 2;
-  for (int i = threadIdx.x; i < 2 * kSelBins; i += blockDim.x) h[i / kSelBins][i % kSelBins] = 0u;
-  __syncthreads();
-  const int hi = shift + width;
-  const uint64_t dmask = (1ULL << width) - 1ULL;
-  const int64_t stride = static_cast<int64_t>(nblk) * blockDim.x;
-  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < a.items; t += stride) {
-    double v;
-    if (!sel_item(g, a, b, t, &v)) continue;
-    const uint64_t k = sel_key(v);
-    const uint32_t bin = static_cast<uint32_t>((k >> shift) & dmask);
-    if (first) {
-      atomicAdd(&h[0][bin], 1u);
-    } else {
-      if ((k >> hi) == (S.prefix[0] >> hi)) atomicAdd(&h[0][bin], 1u);
-      if (nr == 2 && (k >> hi) == (S.prefix[1] >> hi)) atomicAdd(&h[1][bin], 1u);
-    }
-  }
-  __syncthreads();
-  const int nb = 1 << width;
-  for (int i = threadIdx.x; i < nr * nb; i += blockDim.x) {
-    const int r = i / nb, bin = i % nb;
-    const uint32_t c = h[r][bin];
-    if (c) atomicAdd(reinterpret_cast<unsigned long long*>(&hist[(b * 2 + r) * kSelBins + bin]), static_cast<unsigned long long>(c));
-  }
-}
+template <class K>
+struct SelLeader {
+  K prefix[2];
+  unsigned long long rank[2];
+  long long count;
+  double gamma;
+  int32_t live, same;
+};
 
-// NumPy's linear quantile index ((n - 1) q; ends clamped) and the end-exact lerp.
-__device__ __forceinline__ void q_index(int64_t n, double q, int64_t* i, int64_t* j, double* gamma) {
-  const double v = __dmul_rn(static_cast<double>(n - 1), q);
-  if (v >= static_cast<double>(n - 1)) {
-    *i = *j = n - 1;
-    *gamma = __dadd_rn(v, 1.0);
-  } else if (v < 0.0) {
-    *i = *j = 0;
-    *gamma = v;
-  } else {
-    const double fl = floor(v);
-    *i = static_cast<int64_t>(fl);
-    *j = *i + 1;
-    *gamma = __dsub_rn(v, fl);
-  }
-}
-__device__ __forceinline__ double q_lerp(double a, double b, double gamma) {
-  const double diff = __dsub_rn(b, a);
-  return gamma >= 0.5 ? __dsub_rn(b, __dmul_rn(diff, __dsub_rn(1.0, gamma))) : __dadd_rn(a, __dmul_rn(diff, gamma));
-}
-
-__global__ void __launch_bounds__(kThreads) sel_pick(const int32_t* run, SelState* st, uint64_t* hist, int32_t shift,
-                                                     int32_t width, int32_t first, double q) {
-  __shared__ uint64_t part[kThreads];
-  __shared__ uint64_t base[kThreads];
-  __shared__ SelState S;
-  __shared__ int32_t found_bin;
-  __shared__ uint64_t found_rank;
-  const int64_t b = blockIdx.x;
-  if (run && !run[b]) return;
-  const int tid = threadIdx.x;
-  if (tid == 0) S = st[b];
-  __syncthreads();
-  if (!first && !S.valid) return;
-  const int nb = 1 << width;
+// The digit value of table tb (nb bins) that holds rank, and the rank inside it: one block-wide
+// exclusive prefix sum over the bins (nb / kThreads consecutive bins per thread).
+__device__ __forceinline__ void rank_digit(const unsigned long long* tb, int nb, unsigned long long rank,
+                                           unsigned long long* warp_tot, int* bin_out,
+                                           unsigned long long* rest_out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int per = nb / kThreads;
-  uint64_t* h0 = hist + (b * 2) * kSelBins;
-  if (first) {
-    uint64_t sum = 0;
-    for (int j = 0; j < per; ++j) sum += h0[tid * per + j];
-    part[tid] = sum;
-    __syncthreads();
-    if (tid == 0) {
-      uint64_t n = 0;
-      for (int t = 0; t < kThreads; ++t) n += part[t];
-      S.count = static_cast<int64_t>(n);
-      S.valid = n > 0;
-      S.prefix[0] = S.prefix[1] = 0;
-      S.same = 1;
-      if (n > 0) {
-        if (q < 0) {
-          S.rank[0] = (n - 1) / 2;
-          S.rank[1] = n / 2;
-        } else {
-          int64_t i = 0, j = 0;
-          double gm = 0.0;
-          q_index(static_cast<int64_t>(n), q, &i, &j, &gm);
-          S.gamma = gm;
-          S.rank[0] = static_cast<uint64_t>(i);
-          S.rank[1] = static_cast<uint64_t>(j);
-        }
+  unsigned long long mine = 0;
+  for (int j = 0; j < per; ++j) mine += tb[tid * per + j];
+  unsigned long long incl = mine;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long o = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += o;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  unsigned long long before = incl - mine;
+  for (int w = 0; w < warp; ++w) before += warp_tot[w];
+  if (rank >= before && rank < before + mine) {
+    unsigned long long acc = before;
+    for (int j = 0; j < per; ++j) {
+      const unsigned long long c = tb[tid * per + j];
+      if (rank < acc + c) {
+        *bin_out = tid * per + j;
+        *rest_out = rank - acc;
+        break;
       }
-    }
-    __syncthreads();
-    if (!S.valid) {
-      if (tid == 0) st[b] = S;
-      return;
+      acc += c;
     }
   }
-  for (int r = 0; r < 2; ++r) {
-    const uint64_t* hr = hist + (b * 2 + (S.same ? 0 : r)) * kSelBins;
-    uint64_t sum = 0;
-    for (int j = 0; j < per; ++j) sum += hr[tid * per + j];
-    part[tid] = sum;
-    __syncthreads();
-    if (tid == 0) {
-      uint64_t acc = 0;
-      for (int t = 0; t < kThreads; ++t) {
-        base[t] = acc;
-        acc += part[t];
-      }
-    }
-    __syncthreads();
-    const uint64_t rank = S.rank[r];
-    if (rank >= base[tid] && rank < base[tid] + part[tid]) {
-      uint64_t acc = base[tid];
-      for (int j = 0; j < per; ++j) {
-        const uint64_t c = hr[tid * per + j];
-        if (rank < acc + c) {
-          found_bin = tid * per + j;
-          found_rank = rank - acc;
-          break;
-        }
-        acc += c;
-      }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      S.prefix[r] |= static_cast<uint64_t>(found_bin) << shift;
-      S.rank[r] = found_rank;
-    }
-    __syncthreads();
-  }
-  for (int i = tid; i < 2 * kSelBins; i += kThreads) h0[i] = 0;
-  if (tid == 0) {
-    S.same = S.prefix[0] == S.prefix[1];
-    st[b] = S;
-  }
+  __syncthreads();
 }
 
-// low: key bits below the last digit the passes resolved; every item sharing the resolved prefix
-// has the same low bits (float values: zeros for keys of non-negative values, ones for negative).
-__global__ void sel_final(int64_t B, const int32_t* run, const SelState* st, double q, double* out, int64_t* count,
-                          int32_t low) {
-  const int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (b >= B || (run && !run[b])) return;
-  const SelState S = st[b];
-  if (count) count[b] = S.valid ? S.count : 0;
-  if (!S.valid) {
-    out[b] = d_nan();
-    return;
+// NumPy's "linear" quantile: the index (n - 1) q, clamped at the ends, and its fraction.
+__device__ __forceinline__ void linear_index(long long n, double q, long long* i, long long* j, double* frac) {
+  const double pos = __dmul_rn(static_cast<double>(n - 1), q);
+  if (pos >= static_cast<double>(n - 1)) {
+    *i = *j = n - 1;
+    *frac = __dadd_rn(pos, 1.0);
+  } else if (pos < 0.0) {
+    *i = *j = 0;
+    *frac = pos;
+  } else {
+    const double whole = floor(pos);
+    *i = static_cast<long long>(whole);
+    *j = *i + 1;
+    *frac = __dsub_rn(pos, whole);
   }
-  const uint64_t lm = low > 0 ? (1ULL << low) - 1ULL : 0ULL;
-  const double a = sel_value(S.prefix[0] | ((S.prefix[0] >> 63) ? 0ULL : lm));
-  const double c = sel_value(S.prefix[1] | ((S.prefix[1] >> 63) ? 0ULL : lm));
-  if (q < 0) out[b] = S.count % 2 ? a : (a + c) / 2.0;
-  else out[b] = q_lerp(a, c, S.gamma);
+}
+// NumPy's interpolation between neighbours: from the nearer end.
+__device__ __forceinline__ double linear_between(double lo, double hi, double frac) {
+  const double span = __dsub_rn(hi, lo);
+  if (frac >= 0.5) return __dsub_rn(hi, __dmul_rn(span, __dsub_rn(1.0, frac)));
+  return __dadd_rn(lo, __dmul_rn(span, frac));
 }
 
-__global__ void sel_init(int64_t B, const int32_t* run, SelState* st, uint64_t* hist) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= B * 2 * kSelBins) return;
-  const int64_t b = i / (2 * kSelBins);
-  if (run && !run[b]) return;
-  hist[i] = 0;
-  if (i % (2 * kSelBins) == 0) st[b] = SelState{};
+template <class T, class K>
+__global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a, const int32_t* run, double q,
+                                                          double* out, int64_t* count_out) {
+  constexpr int kKeyBits = 8 * static_cast<int>(sizeof(K));
+  constexpr int kDigits = (kKeyBits + kDigitBits - 1) / kDigitBits;
+  extern __shared__ __align__(16) unsigned char sel_smem[];
+  auto* table = reinterpret_cast<unsigned long long*>(sel_smem);                                  // leader: [2][bins]
+  auto* local = reinterpret_cast<uint32_t*>(sel_smem + 2 * kDigitBins * sizeof(unsigned long long));  // [2][bins]
+  __shared__ SelLeader<K> lead;
+  __shared__ unsigned long long warp_tot[kThreads / 32];
+  __shared__ int hit_bin;
+  __shared__ unsigned long long hit_rest;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned me = cl.block_rank();
+  const unsigned ctas = cl.num_blocks();
+  const int64_t b = blockIdx.y;
+  if (run && !run[b]) return;  // every CTA of the cluster leaves here
+  const int tid = threadIdx.x;
+  const bool leader = me == 0;
+  SelLeader<K>* L = cl.map_shared_rank(&lead, 0);
+  unsigned long long* T0 = cl.map_shared_rank(table, 0);
+  if (leader) {
+    for (int i = tid; i < 2 * kDigitBins; i += kThreads) table[i] = 0ULL;
+    if (tid == 0) {
+      lead.prefix[0] = lead.prefix[1] = K(0);
+      lead.live = 1;
+      lead.same = 1;
+    }
+  }
+  for (int pass = 0; pass < kDigits; ++pass) {
+    const int hi = kKeyBits - kDigitBits * pass;  // key bits at and above hi are resolved
+    const int shift = hi > kDigitBits ? hi - kDigitBits : 0;
+    const int width = hi - shift;
+    const K dmask = static_cast<K>((K(1) << width) - K(1));
+    for (int i = tid; i < 2 * kDigitBins; i += kThreads) local[i] = 0u;
+    cl.sync();  // the leader's prefixes and cleared table are visible to the cluster
+    const int live = L->live;
+    if (!live) break;
+    const bool two = pass > 0 && !L->same;
+    const K p0 = L->prefix[0], p1 = L->prefix[1];
+    const int64_t stride = static_cast<int64_t>(ctas) * kThreads;
+    for (int64_t t = static_cast<int64_t>(me) * kThreads + tid; t < a.items; t += stride) {
+      K k;
+      if (!sel_key_of<T, K>(g, a, b, t, &k)) continue;
+      const uint32_t digit = static_cast<uint32_t>((k >> shift) & dmask);
+      if (pass == 0) {
+        atomicAdd(&local[digit], 1u);
+        continue;
+      }
+      const K top = k >> hi;
+      if (top == (p0 >> hi)) atomicAdd(&local[digit], 1u);
+      if (two && top == (p1 >> hi)) atomicAdd(&local[kDigitBins + digit], 1u);
+    }
+    __syncthreads();
+    const int bins = 1 << width;
+    for (int i = tid; i < (two ? 2 : 1) * bins; i += kThreads) {
+      const int r = i >= bins ? 1 : 0;
+      const uint32_t c = local[r * kDigitBins + (i - r * bins)];
+      if (c) atomicAdd(&T0[r * kDigitBins + (i - r * bins)], static_cast<unsigned long long>(c));
+    }
+    cl.sync();  // the cluster's counts are complete in the leader's table
+    if (!leader) continue;
+    if (pass == 0) {
+      // the item count and the ranks of the statistic
+      unsigned long long n = 0;
+      for (int i = tid; i < bins; i += kThreads) n += table[i];
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) n += __shfl_xor_sync(0xffffffffu, n, d);
+      if ((tid & 31) == 0) warp_tot[tid >> 5] = n;
+      __syncthreads();
+      if (tid == 0) {
+        unsigned long long total = 0;
+        for (int w = 0; w < kThreads / 32; ++w) total += warp_tot[w];
+        lead.count = static_cast<long long>(total);
+        lead.live = total > 0;
+        if (total > 0) {
+          if (q < 0) {
+            lead.rank[0] = (total - 1) / 2;
+            lead.rank[1] = total / 2;
+          } else {
+            long long i = 0, j = 0;
+            linear_index(static_cast<long long>(total), q, &i, &j, &lead.gamma);
+            lead.rank[0] = static_cast<unsigned long long>(i);
+            lead.rank[1] = static_cast<unsigned long long>(j);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (lead.live) {
+      for (int r = 0; r < 2; ++r) {
+        rank_digit(table + (two ? r : 0) * kDigitBins, bins, lead.rank[r], warp_tot, &hit_bin, &hit_rest);
+        if (tid == 0) {
+          lead.prefix[r] |= static_cast<K>(hit_bin) << shift;
+          lead.rank[r] = hit_rest;
+        }
+        __syncthreads();
+      }
+      if (tid == 0) lead.same = lead.prefix[0] == lead.prefix[1];
+    }
+    for (int i = tid; i < 2 * kDigitBins; i += kThreads) table[i] = 0ULL;
+  }
+  cl.sync();  // no CTA reads the leader's shared memory after this
+  if (leader && tid == 0) {
+    if (!lead.live) {
+      out[b] = d_nan();
+      if (count_out) count_out[b] = 0;
+    } else {
+      const double v0 = key_value(lead.prefix[0]), v1 = key_value(lead.prefix[1]);
+      out[b] = q < 0 ? ((lead.count & 1) ? v0 : __dmul_rn(__dadd_rn(v0, v1), 0.5)) : linear_between(v0, v1, lead.gamma);
+      if (count_out) count_out[b] = lead.count;
+    }
+  }
 }
 
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
@@ -410,14 +437,11 @@ void field_totals(cudaStream_t s, const Geom& g, const T* f, double* energy, dou
   EDAB_LAUNCH("element_totals");
 }
 
-size_t select_scratch_bytes(const Geom& g) {
-  return align256(static_cast<size_t>(g.batch) * sizeof(SelState)) +
-         align256(static_cast<size_t>(g.batch) * 2 * kSelBins * sizeof(uint64_t));
-}
+size_t select_scratch_bytes(const Geom&) { return 0; }
 
 template <class T>
 void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const int32_t* run, double* out,
-            int64_t* count, void* scratch) {
+            int64_t* count, void*) {
   SelView<T> a{};
   a.sel = sel;
   if (sel.src == SelSrc::kField) {
@@ -429,31 +453,36 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
     }
     a.items = static_cast<int64_t>(a.naxes) * g.field;
   }
-  const int64_t B = g.batch;
-  auto* st = static_cast<SelState*>(scratch);
-  auto* hist = reinterpret_cast<uint64_t*>(static_cast<char*>(scratch) + align256(static_cast<size_t>(B) * sizeof(SelState)));
-  sel_init<<<blocks_for(B * 2 * kSelBins), kThreads, 0, s>>>(B, run, st, hist);
-  EDAB_LAUNCH("sel_init");
-  int64_t nblk = (a.items + int64_t{kThreads} * 32 - 1) / (int64_t{kThreads} * 32);
-  nblk = std::clamp<int64_t>(nblk, 1, 1024);
-  if (B > 65535) throw std::invalid_argument("edab: select batch too large");
-  // float items (a float32 field or its float32 differences, no centre) have double keys whose low
-  // 29 bits depend only on the sign: four passes resolve every bit above bit 20
-  const int passes = std::is_same_v<T, float> && sel.center == nullptr ? 4 : kSelPasses;
-  int low = 0;
-  for (int p = 0; p < passes; ++p) {
-    const int top = 64 - kSelBits * p;
-    const int shift = top - kSelBits > 0 ? top - kSelBits : 0;
-    const int width = top - shift;
-    sel_hist<T><<<dim3(static_cast<unsigned>(nblk), static_cast<unsigned>(B)), kThreads, 0, s>>>(
-        g, a, run, st, hist, static_cast<int32_t>(nblk), shift, width, p == 0);
-    EDAB_LAUNCH("sel_hist");
-    sel_pick<<<static_cast<unsigned>(B), kThreads, 0, s>>>(run, st, hist, shift, width, p == 0, q);
-    EDAB_LAUNCH("sel_pick");
-    low = shift;
+  if (g.batch > 65535) throw std::invalid_argument("edab: select batch too large");
+  // CTAs per element: about 16 items per thread, up to a cluster of 8
+  const int64_t per_cta = int64_t{kThreads} * 16;
+  const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>((a.items + per_cta - 1) / per_cta, 1, kSelClusterMax));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(ctas, static_cast<unsigned>(g.batch));
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSelSmem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const auto launch = [&](auto kernel) {
+    if (first_on_device(reinterpret_cast<const void*>(kernel))) {
+      EDAB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSelSmem)));
+    }
+    EDAB_CUDA(cudaLaunchKernelEx(&cfg, kernel, g, a, run, q, out, count));
+    EDAB_LAUNCH("select_cluster");
+  };
+  if constexpr (std::is_same_v<T, float>) {
+    if (sel.center == nullptr) {
+      launch(select_cluster<T, uint32_t>);
+      return;
+    }
   }
-  sel_final<<<blocks_for(B), kThreads, 0, s>>>(B, run, st, q, out, count, low);
-  EDAB_LAUNCH("sel_final");
+  launch(select_cluster<T, uint64_t>);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -466,22 +495,12 @@ namespace {
 
 constexpr int kBlk = 32;
 
-// fl64(a - b) >= tau: for float the float difference decides except on a tie with tau.
+// A drop from hi to lo is significant when fl64(hi - lo) >= tau: the difference of the two samples
+// in double, rounded once. (For float32 samples the float difference decides the same way except on
+// an exact tie with tau; the double difference settles every case with one rule.)
 template <class T>
-__device__ __forceinline__ bool deep(T a, T b, T tau) {
-  if constexpr (std::is_same_v<T, float>) {
-    const float d = __fsub_rn(a, b);
-    if (d != tau) return d > tau;
-    return __dsub_rn(static_cast<double>(a), static_cast<double>(b)) >= static_cast<double>(tau);
-  } else {
-    return __dsub_rn(a, b) >= tau;
-  }
-}
-
-template <bool Max, class T>
-__device__ __forceinline__ int side_step(T u, T v, T tau) {
-  if (Max ? !(u <= v) : !(u >= v)) return 2;
-  return (Max ? deep<T>(v, u, tau) : deep<T>(u, v, tau)) ? 1 : 0;
+__device__ __forceinline__ bool drops(T hi, T lo, T tau) {
+  return __dsub_rn(static_cast<double>(hi), static_cast<double>(lo)) >= static_cast<double>(tau);
 }
 
 // Sample k of a staged line: one pad word after every 32 samples (the lanes of a warp scanning
@@ -491,28 +510,41 @@ __device__ __forceinline__ T xs(const T* x, int32_t k) {
   return x[k + (k >> 5)];
 }
 
+// Samples k = from, from + Dir, .. to of a staged line against the peak value v: 1 when a sample
+// lies a significant drop away from v before any sample lies beyond v (above a maximum, below a
+// minimum, or NaN), 0 when a sample beyond v comes first, -1 when the range holds neither.
 template <bool Max, int Dir, class T>
-__device__ bool side_deep(const T* x, int32_t n, int32_t p, T v, T tau, const T* bmin, const T* bmax) {
-  const int32_t cp = p / kBlk;
-  const int32_t lim = Dir < 0 ? cp * kBlk : min(cp * kBlk + kBlk - 1, n - 1);
-  for (int32_t k = p + Dir; Dir < 0 ? k >= lim : k <= lim; k += Dir) {
-    const int st = side_step<Max>(xs(x, k), v, tau);
-    if (st) return st == 1;
+__device__ __forceinline__ int walk_samples(const T* x, int32_t from, int32_t to, T v, T tau) {
+  for (int32_t k = from; (to - k) * Dir >= 0; k += Dir) {
+    const T u = xs(x, k);
+    if (Max ? !(u <= v) : !(u >= v)) return 0;
+    if (Max ? drops(v, u, tau) : drops(u, v, tau)) return 1;
   }
-  const int32_t nb = (n + kBlk - 1) / kBlk;
-  for (int32_t c = cp + Dir; Dir < 0 ? c >= 0 : c < nb; c += Dir) {
-    const T hi = Max ? bmax[c] : bmin[c];
-    if (Max ? !(hi <= v) : !(hi >= v)) {
-      const int32_t k0 = Dir < 0 ? c * kBlk + kBlk - 1 : c * kBlk;
-      const int32_t k1 = Dir < 0 ? c * kBlk : min(c * kBlk + kBlk - 1, n - 1);
-      for (int32_t k = k0; Dir < 0 ? k >= k1 : k <= k1; k += Dir) {
-        const int st = side_step<Max>(xs(x, k), v, tau);
-        if (st) return st == 1;
-      }
-      return false;
+  return -1;
+}
+
+// Whether the side of the peak at p (value v) in direction Dir falls by tau before it rises beyond
+// v (the line end counts as no fall): SciPy's prominence base on that side is at least tau below
+// the peak. The rest of the peak's 32-sample block is walked sample by sample; then every block is
+// judged by its extremes (bext: the extreme towards "beyond", bnear: the other one): a block with
+// nothing beyond v either holds a significant drop or is passed over; the first block with a sample
+// beyond v is walked and decides.
+template <bool Max, int Dir, class T>
+__device__ bool side_falls(const T* x, int32_t n, int32_t p, T v, T tau, const T* bext, const T* bnear) {
+  const int32_t blocks = (n + kBlk - 1) / kBlk;
+  int32_t c = p / kBlk;
+  const int32_t edge = Dir > 0 ? min(c * kBlk + kBlk - 1, n - 1) : c * kBlk;
+  if ((edge - p) * Dir > 0) {
+    const int verdict = walk_samples<Max, Dir>(x, p + Dir, edge, v, tau);
+    if (verdict >= 0) return verdict == 1;
+  }
+  for (c += Dir; c >= 0 && c < blocks; c += Dir) {
+    const T e = bext[c];
+    if (Max ? !(e <= v) : !(e >= v)) {
+      const int32_t first = c * kBlk, last = min(first + kBlk - 1, n - 1);
+      return walk_samples<Max, Dir>(x, Dir > 0 ? first : last, Dir > 0 ? last : first, v, tau) == 1;
     }
-    const T lo = Max ? bmin[c] : bmax[c];
-    if (Max ? deep<T>(v, lo, tau) : deep<T>(lo, v, tau)) return true;
+    if (Max ? drops(v, bnear[c], tau) : drops(bnear[c], v, tau)) return true;
   }
   return false;
 }
@@ -632,8 +664,8 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
     const int32_t pk = (s + e) / 2;
     const int64_t at = eoff + base_s[p] + pk * step;
     const T tp = pk == s ? tp_s : tau[at];
-    const bool sig = is_max ? side_deep<true, -1>(x, n, pk, cur, tp, pmin, pmax) && side_deep<true, 1>(x, n, pk, cur, tp, pmin, pmax)
-                            : side_deep<false, -1>(x, n, pk, cur, tp, pmin, pmax) && side_deep<false, 1>(x, n, pk, cur, tp, pmin, pmax);
+    const bool sig = is_max ? side_falls<true, -1>(x, n, pk, cur, tp, pmax, pmin) && side_falls<true, 1>(x, n, pk, cur, tp, pmax, pmin)
+                            : side_falls<false, -1>(x, n, pk, cur, tp, pmin, pmax) && side_falls<false, 1>(x, n, pk, cur, tp, pmin, pmax);
     if (sig) {
       flags[at] |= static_cast<uint8_t>(1u << axis);
       ++mine;
@@ -662,31 +694,72 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
 }
 
 // ---------------------------------------------------------------------------------------------
-// Face-connected components: union-find over the padded in-element indices with atomicMin links
-// (a parent is always smaller than its child), so the root of a component is its smallest index
-// whatever the order of the atomics; a final pass writes every voxel's root.
-__device__ __forceinline__ int32_t find_root(const int32_t* L, int32_t x) {
-  const volatile int32_t* V = L;
-  int32_t p = V[x];
-  while (p != x) {
-    x = p;
-    p = V[x];
-  }
-  return x;
-}
-__device__ __forceinline__ void unite(int32_t* L, int32_t a, int32_t c) {
+// Face-connected components, labelled by the smallest padded index of the component. Parent links
+// always point to a smaller index and a root is linked only by a compare-and-swap that finds it
+// still a root, so every tree's root is its smallest member whatever the order of the threads.
+// Phase 1 labels the components of every tile (consecutive rows of an element) in shared memory;
+// phase 2 joins the trees across the tile borders in global memory; phase 3 points every voxel at
+// its root.
+
+// Root of x; parent reads bypass L1 (another SM may have relinked a root), shared memory is
+// coherent inside the CTA and read volatile.
+template <bool Global>
+__device__ __forceinline__ int32_t uf_root(int32_t* P, int32_t x) {
   for (;;) {
-    a = find_root(L, a);
-    c = find_root(L, c);
-    if (a == c) return;
-    if (a > c) {
-      const int32_t t = a;
-      a = c;
-      c = t;
+    const int32_t up = Global ? __ldcg(P + x) : *reinterpret_cast<volatile int32_t*>(P + x);
+    if (up == x) return x;
+    x = up;
+  }
+}
+template <bool Global>
+__device__ __forceinline__ void uf_join(int32_t* P, int32_t x, int32_t y) {
+  for (;;) {
+    x = uf_root<Global>(P, x);
+    y = uf_root<Global>(P, y);
+    if (x == y) return;
+    const int32_t big = x > y ? x : y, small = x > y ? y : x;
+    if (atomicCAS(P + big, big, small) == big) return;  // big was still a root: now under small
+    x = big;
+    y = small;
+  }
+}
+
+constexpr int32_t kTileWords = 8192;  // int32 parents per tile (32 KiB of shared memory)
+
+__device__ __forceinline__ int64_t rows_between(const Geom& g, int a) { return geom_stride(g, a) / g.pitch; }
+
+__global__ void __launch_bounds__(kThreads) ccl_tiles(Geom g, const uint8_t* __restrict__ mask, uint8_t bits,
+                                                     int32_t* __restrict__ labels, const int32_t* run, int32_t tile_rows) {
+  __shared__ int32_t P[kTileWords];
+  const int64_t b = blockIdx.y;
+  if (run && !run[b]) return;
+  const int64_t row0 = static_cast<int64_t>(blockIdx.x) * tile_rows;
+  if (row0 >= g.rows) return;
+  const int32_t rows = static_cast<int32_t>(min(static_cast<int64_t>(tile_rows), g.rows - row0));
+  const int32_t pitch = static_cast<int32_t>(g.pitch), nl = g.n_last;
+  const int32_t words = rows * pitch;
+  const int64_t v0 = row0 * g.pitch;  // the tile's first padded offset in the element
+  const int64_t base = b * g.field + v0;
+  for (int32_t k = threadIdx.x; k < words; k += blockDim.x) {
+    const int32_t col = k % pitch;
+    P[k] = (col < nl && (mask[base + k] & bits) != 0) ? k : -1;
+  }
+  __syncthreads();
+  for (int32_t k = threadIdx.x; k < words; k += blockDim.x) {
+    if (P[k] < 0) continue;
+    const int32_t r = k / pitch, col = k - r * pitch;
+    if (col + 1 < nl && P[k + 1] >= 0) uf_join<false>(P, k, k + 1);
+    for (int a = 0; a + 1 < g.dim; ++a) {
+      const int64_t rs = rows_between(g, a);
+      if (r + rs >= rows || coord_of(g, v0 + k, a) + 1 >= geom_n(g, a)) continue;
+      const int32_t u = k + static_cast<int32_t>(rs) * pitch;
+      if (P[u] >= 0) uf_join<false>(P, k, u);
     }
-    const int32_t old = atomicMin(L + c, a);
-    if (old == c) return;
-    c = old;
+  }
+  __syncthreads();
+  for (int32_t k = threadIdx.x; k < words; k += blockDim.x) {
+    const int32_t lab = P[k] < 0 ? -1 : static_cast<int32_t>(v0) + uf_root<false>(P, k);
+    labels[base + k] = lab;
   }
 }
 
@@ -702,10 +775,8 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
   EDAB_CUDA(cudaGetDevice(&dev));
   EDAB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const size_t cap = static_cast<size_t>(optin) - 2048;
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[sizeof(T) == 8]) {
+  if (first_on_device(reinterpret_cast<const void*>(flags_pass<T>))) {  // the limit is per device
     EDAB_CUDA(cudaFuncSetAttribute(flags_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cap)));
-    attr_set[sizeof(T) == 8] = true;
   }
   for (int a = 0; a < g.dim; ++a) {
     const int32_t n = g.n[a];
@@ -733,35 +804,33 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
 }
 
 void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32_t* labels, const int32_t* run) {
-  const int64_t total = g.batch * g.field;
-  for_samples(s, total, [=] __device__(int64_t i) {
-    const int64_t b = elem_of(g, i);
-    if (run && !run[b]) return;
-    const int64_t v = i - b * g.field;
-    labels[i] = (!is_pad(g, v) && (mask[i] & bits) != 0) ? static_cast<int32_t>(v) : -1;
-  });
-  for_samples(s, total, [=] __device__(int64_t i) {
-    const int64_t b = elem_of(g, i);
-    if (run && !run[b]) return;
-    int32_t* L = labels + b * g.field;
-    const int32_t v = static_cast<int32_t>(i - b * g.field);
-    if (L[v] < 0) return;
-    for (int a = 0; a < g.dim; ++a) {
-      if (coord_of(g, v, a) + 1 >= geom_n(g, a)) continue;
-      const int32_t u = v + static_cast<int32_t>(a == g.dim - 1 ? 1 : geom_stride(g, a));
-      if (L[u] < 0) continue;
-      unite(L, v, u);
-    }
-  });
-  for_samples(s, total, [=] __device__(int64_t i) {
-    const int64_t b = elem_of(g, i);
-    if (run && !run[b]) return;
-    int32_t* L = labels + b * g.field;
-    const int32_t v = static_cast<int32_t>(i - b * g.field);
-    if (L[v] < 0) return;
-    const int32_t root = find_root(L, v);
-    reinterpret_cast<volatile int32_t*>(L)[v] = root;
-  });
+  const int32_t tile_rows = static_cast<int32_t>(std::max<int64_t>(1, kTileWords / g.pitch));
+  const int64_t tiles = (g.rows + tile_rows - 1) / tile_rows;
+  if (tiles > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: components: grid too large");
+  ccl_tiles<<<dim3(static_cast<unsigned>(tiles), static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(
+      g, mask, bits, labels, run, tile_rows);
+  EDAB_LAUNCH("ccl_tiles");
+  // the edges between tiles
+  for_voxels(s, g, [=] __device__(int64_t b) { return run == nullptr || run[b] != 0; },
+             [=] __device__(int64_t b, int64_t v, int64_t i) {
+               int32_t* L = labels + b * g.field;
+               if (L[v] < 0) return;
+               const int64_t row = pitch_row(g, v);
+               const int64_t tile = row / tile_rows;
+               for (int a = 0; a + 1 < g.dim; ++a) {
+                 const int64_t rs = geom_stride(g, a) / g.pitch;
+                 if ((row + rs) / tile_rows == tile || coord_of(g, v, a) + 1 >= geom_n(g, a)) continue;
+                 const int64_t u = v + geom_stride(g, a);
+                 if (L[u] >= 0) uf_join<true>(L, static_cast<int32_t>(v), static_cast<int32_t>(u));
+               }
+             });
+  // every voxel to its root
+  for_voxels(s, g, [=] __device__(int64_t b) { return run == nullptr || run[b] != 0; },
+             [=] __device__(int64_t b, int64_t v, int64_t i) {
+               int32_t* L = labels + b * g.field;
+               if (L[v] < 0) return;
+               L[v] = uf_root<true>(L, static_cast<int32_t>(v));
+             });
 }
 
 template void field_totals<float>(cudaStream_t, const Geom&, const float*, double*, double*, uint64_t*, void*);

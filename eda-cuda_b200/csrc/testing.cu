@@ -123,6 +123,127 @@ void run_transform(const void* x_dev, int dim, int64_t batch, const int64_t* n, 
   if (herr) throw std::runtime_error("eda_testing_transform: the tensor-core pass gave up waiting for its pipeline");
 }
 
+template <class T>
+void run_select(const void* x_dev, int dim, int64_t batch, const int64_t* n, int src, int axes, const uint8_t* mask_dev,
+                int bits, const double* center, double q, double* out, int64_t* count, cudaStream_t s) {
+  const Geom g = make_geom(dim, batch, n);
+  const int64_t fe = batch * g.field;
+  T* f = nullptr;
+  uint8_t* m = nullptr;
+  double *c = nullptr, *o = nullptr;
+  int64_t* k = nullptr;
+  EDAB_CUDA(cudaMalloc(&f, fe * sizeof(T)));
+  EDAB_CUDA(cudaMalloc(&o, sizeof(double) * batch));
+  EDAB_CUDA(cudaMalloc(&k, sizeof(int64_t) * batch));
+  to_padded<T><<<std::min(blocks_for(fe), 1u << 16), kThreads, 0, s>>>(g, static_cast<const T*>(x_dev), f);
+  EDAB_LAUNCH("to_padded");
+  if (mask_dev) {
+    EDAB_CUDA(cudaMalloc(&m, fe));
+    to_padded<uint8_t><<<std::min(blocks_for(fe), 1u << 16), kThreads, 0, s>>>(g, mask_dev, m);
+    EDAB_LAUNCH("to_padded");
+  }
+  if (center) {
+    EDAB_CUDA(cudaMalloc(&c, sizeof(double) * batch));
+    EDAB_CUDA(cudaMemcpyAsync(c, center, sizeof(double) * batch, cudaMemcpyHostToDevice, s));
+  }
+  Sel<T> sel{};
+  sel.src = src == 0 ? SelSrc::kField : SelSrc::kDiff;
+  sel.field = f;
+  sel.mask = m;
+  sel.bits = static_cast<uint8_t>(bits);
+  sel.axes = static_cast<uint8_t>(axes);
+  sel.center = c;
+  select<T>(s, g, sel, q, nullptr, o, k, nullptr);
+  EDAB_CUDA(cudaMemcpyAsync(out, o, sizeof(double) * batch, cudaMemcpyDeviceToHost, s));
+  if (count) EDAB_CUDA(cudaMemcpyAsync(count, k, sizeof(int64_t) * batch, cudaMemcpyDeviceToHost, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+  cudaFree(f);
+  cudaFree(m);
+  cudaFree(c);
+  cudaFree(o);
+  cudaFree(k);
+}
+
+template <class T>
+void run_flags(const void* r_dev, const void* tau_dev, int dim, int64_t batch, const int64_t* n, uint8_t* flags_dev,
+               uint64_t* ext, cudaStream_t s) {
+  const Geom g = make_geom(dim, batch, n);
+  const int64_t fe = batch * g.field;
+  T *r = nullptr, *tau = nullptr;
+  uint8_t* fl = nullptr;
+  Elem* el = nullptr;
+  EDAB_CUDA(cudaMalloc(&r, fe * sizeof(T)));
+  EDAB_CUDA(cudaMalloc(&tau, fe * sizeof(T)));
+  EDAB_CUDA(cudaMalloc(&fl, fe));
+  EDAB_CUDA(cudaMalloc(&el, sizeof(Elem) * batch));
+  EDAB_CUDA(cudaMemsetAsync(el, 0, sizeof(Elem) * batch, s));
+  EDAB_CUDA(cudaMemsetAsync(fl, 0xff, fe, s));  // the pass clears the flags of the running elements itself
+  const unsigned blocks = std::min(blocks_for(fe), 1u << 16);
+  to_padded<T><<<blocks, kThreads, 0, s>>>(g, static_cast<const T*>(r_dev), r);
+  EDAB_LAUNCH("to_padded");
+  to_padded<T><<<blocks, kThreads, 0, s>>>(g, static_cast<const T*>(tau_dev), tau);
+  EDAB_LAUNCH("to_padded");
+  sig_flags<T>(s, g, r, tau, fl, el, nullptr);
+  to_dense<uint8_t><<<std::min(blocks_for(batch * g.count), 1u << 16), kThreads, 0, s>>>(g, batch, fl, flags_dev);
+  EDAB_LAUNCH("to_dense");
+  std::vector<Elem> h(static_cast<size_t>(batch));
+  EDAB_CUDA(cudaMemcpyAsync(h.data(), el, sizeof(Elem) * batch, cudaMemcpyDeviceToHost, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+  for (int64_t b = 0; b < batch; ++b) {
+    for (int a = 0; a < dim; ++a) ext[b * dim + a] = h[static_cast<size_t>(b)].ext[a];
+  }
+  cudaFree(r);
+  cudaFree(tau);
+  cudaFree(fl);
+  cudaFree(el);
+}
+
+// padded labels (the smallest padded index of the component) to dense ones (its dense index)
+__global__ void labels_dense(Geom g, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
+  const int32_t nl = g.n_last;
+  const int64_t total = g.batch * g.count;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = i / g.count, c = i - b * g.count;
+    const int64_t row = c / nl, col = c - row * nl;
+    const int32_t v = lab[b * g.field + row * g.pitch + col];
+    out[i] = v < 0 ? -1 : static_cast<int32_t>((v / g.pitch) * nl + v % g.pitch);
+  }
+}
+
+void run_components(const uint8_t* mask_dev, int bits, int dim, int64_t batch, const int64_t* n, int32_t* labels_dev,
+                    cudaStream_t s) {
+  const Geom g = make_geom(dim, batch, n);
+  const int64_t fe = batch * g.field;
+  uint8_t* m = nullptr;
+  int32_t* lab = nullptr;
+  EDAB_CUDA(cudaMalloc(&m, fe));
+  EDAB_CUDA(cudaMalloc(&lab, fe * sizeof(int32_t)));
+  to_padded<uint8_t><<<std::min(blocks_for(fe), 1u << 16), kThreads, 0, s>>>(g, mask_dev, m);
+  EDAB_LAUNCH("to_padded");
+  ccl(s, g, m, static_cast<uint8_t>(bits), lab, nullptr);
+  labels_dense<<<std::min(blocks_for(batch * g.count), 1u << 16), kThreads, 0, s>>>(g, lab, labels_dev);
+  EDAB_LAUNCH("labels_dense");
+  EDAB_CUDA(cudaStreamSynchronize(s));
+  cudaFree(m);
+  cudaFree(lab);
+}
+
+template <class F>
+int guarded(const char* name, F f) {
+  try {
+    f();
+    set_last_error("");
+    return EDA_OK;
+  } catch (const std::invalid_argument& e) {
+    set_last_error(e.what());
+    return EDA_INVALID_ARGUMENT;
+  } catch (const std::exception& e) {
+    set_last_error((std::string(name) + ": " + e.what()).c_str());
+    return EDA_CUDA_ERROR;
+  }
+}
+
 }  // namespace
 
 extern "C" int eda_testing_cube(const void* x_dev, int dtype, int dim, int64_t batch, const int64_t* n, int op,
@@ -171,4 +292,47 @@ extern "C" int eda_testing_transform(const void* x_dev, int dtype, int dim, int6
     set_last_error(e.what());
     return EDA_CUDA_ERROR;
   }
+}
+
+extern "C" int eda_testing_select(const void* x_dev, int dtype, int dim, int64_t batch, const int64_t* n, int src,
+                                  int axes, const uint8_t* mask_dev, int bits, const double* center, double q,
+                                  double* out, int64_t* count, void* stream) {
+  return guarded("eda_testing_select", [&] {
+    if (!x_dev || !n || !out || batch < 1 || dim < 1 || dim > kMaxDim || src < 0 || src > 1 ||
+        (src == 1 && (axes <= 0 || axes >= (1 << dim))) || (src == 0 && mask_dev && (bits <= 0 || bits > 255)) ||
+        (q >= 0 && q > 1)) {
+      throw std::invalid_argument("eda_testing_select: invalid argument");
+    }
+    Params p;
+    validate(dtype, dim, batch, n, p);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == 0) run_select<float>(x_dev, dim, batch, n, src, axes, mask_dev, bits, center, q, out, count, s);
+    else run_select<double>(x_dev, dim, batch, n, src, axes, mask_dev, bits, center, q, out, count, s);
+  });
+}
+
+extern "C" int eda_testing_flags(const void* r_dev, const void* tau_dev, int dtype, int dim, int64_t batch,
+                                 const int64_t* n, uint8_t* flags_dev, uint64_t* ext, void* stream) {
+  return guarded("eda_testing_flags", [&] {
+    if (!r_dev || !tau_dev || !n || !flags_dev || !ext || batch < 1 || dim < 1 || dim > kMaxDim) {
+      throw std::invalid_argument("eda_testing_flags: invalid argument");
+    }
+    Params p;
+    validate(dtype, dim, batch, n, p);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == 0) run_flags<float>(r_dev, tau_dev, dim, batch, n, flags_dev, ext, s);
+    else run_flags<double>(r_dev, tau_dev, dim, batch, n, flags_dev, ext, s);
+  });
+}
+
+extern "C" int eda_testing_components(const uint8_t* mask_dev, int bits, int dim, int64_t batch, const int64_t* n,
+                                      int32_t* labels_dev, void* stream) {
+  return guarded("eda_testing_components", [&] {
+    if (!mask_dev || !n || !labels_dev || batch < 1 || dim < 1 || dim > kMaxDim || bits <= 0 || bits > 255) {
+      throw std::invalid_argument("eda_testing_components: invalid argument");
+    }
+    Params p;
+    validate(0, dim, batch, n, p);
+    run_components(mask_dev, bits, dim, batch, n, labels_dev, static_cast<cudaStream_t>(stream));
+  });
 }

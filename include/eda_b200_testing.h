@@ -35,6 +35,34 @@ EDA_API int eda_testing_cube(const void* x_dev, int dtype, int dim, int64_t batc
 EDA_API int eda_testing_transform(const void* x_dev, int dtype, int dim, int64_t batch, const int64_t* n,
                                   const int32_t* kinds, void* out_dev, void* stream);
 
+/* The exact selection of every element of x_dev (dense (batch, n..), dtype 0 float32 / 1 float64,
+ * on the current device): src 0 selects the samples (those with (mask & bits) != 0 when mask_dev, a
+ * dense u8 array of the same shape, is given), src 1 the forward differences x[i + e_a] - x[i] in the
+ * dtype along every axis a in the bit set `axes`; center (host, [batch], or NULL) selects
+ * |value - center[b]| in double instead. q < 0: NumPy's median; 0 <= q <= 1: NumPy's "linear"
+ * quantile; out (host, [batch]) receives it (NaN for an empty set), count (host, [batch], or NULL)
+ * the number of items. Replaces the harness calls of enqueue_median / enqueue_quantile
+ * (cpp/src/method/stats.cu:221-296; tested in cpp/tests/test_stats.cu:130-326). Synchronizes. */
+EDA_API int eda_testing_select(const void* x_dev, int dtype, int dim, int64_t batch, const int64_t* n, int src,
+                               int axes, const uint8_t* mask_dev, int bits, const double* center, double q,
+                               double* out, int64_t* count, void* stream);
+
+/* The significant extrema of every line of every axis of r_dev against the threshold field tau_dev
+ * (both dense (batch, n..) of the dtype on the current device): flags_dev (dense u8) receives bit a
+ * for an extremum of a line along axis a (SciPy's find_peaks with topographic prominence >= tau at
+ * the peak), ext (host, [batch][dim]) their counts. Replaces the harness calls of enqueue_sig_flags
+ * (cpp/src/method/stats_fields.cu:392-422; tested in cpp/tests/test_stats.cu:436-902). Synchronizes. */
+EDA_API int eda_testing_flags(const void* r_dev, const void* tau_dev, int dtype, int dim, int64_t batch,
+                              const int64_t* n, uint8_t* flags_dev, uint64_t* ext, void* stream);
+
+/* The face-connected components of (mask & bits) != 0 of every element of mask_dev (dense u8
+ * (batch, n..) on the current device): labels_dev (dense int32) receives the smallest dense index
+ * of the sample's component inside its element, -1 outside. Replaces the harness calls of
+ * enqueue_ccl (cpp/src/method/stats_scale.cu:208-220; tested in cpp/tests/test_stats.cu:966-1050).
+ * Synchronizes. */
+EDA_API int eda_testing_components(const uint8_t* mask_dev, int bits, int dim, int64_t batch, const int64_t* n,
+                                   int32_t* labels_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -497,6 +497,10 @@ void orientation_eigen(int D, int64_t N, const std::vector<T>* R1, const std::ve
 }
 
 template <class T>
+void extrema_flags(const Shape& sh, const std::vector<T>& r, const std::vector<T>& tau, std::vector<uint8_t>& flags,
+                   uint64_t* ext);
+
+template <class T>
 class Element {
  public:
   Element(const Shape& sh, const Ctl& c, double tau_rel, bool check_finite, int32_t max_imf, int32_t cap)
@@ -618,6 +622,12 @@ inline bool deep(T a, T b, T tau) {
 
 template <class T>
 void Element<T>::sig_flags(const F& r, const F& tau, std::vector<uint8_t>& flags, uint64_t* ext) const {
+  extrema_flags<T>(sh_, r, tau, flags, ext);
+}
+
+template <class T>
+void extrema_flags(const Shape& sh_, const std::vector<T>& r, const std::vector<T>& tau, std::vector<uint8_t>& flags,
+                   uint64_t* ext) {
   // scipy.signal.find_peaks + peak_prominences >= tau on every line of every axis
   // (cpp/src/method/stats_fields.cu:1-14, 207-331)
   flags.assign(static_cast<size_t>(sh_.count), 0);
@@ -1752,6 +1762,43 @@ int eda_oracle_rung_ladder(double d_min, double d_max, int32_t w, int32_t n_max,
 }
 
 // One cube filter of one element (tests): op 0 max, 1 min, 3 box; f (count values) in place.
+// Stage hooks for the stage-level tests: the exact selection of the doubles v (q < 0: the median;
+// NaN for an empty set), the significant-extrema flags of one element (bit a: axis a) with the
+// counts per axis, and the face-connected components of mask != 0 (label: the smallest index of
+// the component, -1 outside).
+int eda_oracle_select(const double* v, int64_t n, double q, double* out) {
+  std::vector<double> w(v, v + n);
+  *out = q < 0 ? oracle::select_median(w) : oracle::select_quantile(w, q);
+  return 0;
+}
+
+int eda_oracle_flags(int dtype, int dim, const int64_t* n, const void* r, const void* tau, uint8_t* flags,
+                     uint64_t* ext) {
+  const oracle::Shape sh(dim, n);
+  std::vector<uint8_t> f;
+  for (int a = 0; a < 3; ++a) ext[a] = 0;
+  if (dtype == 0) {
+    const auto* rp = static_cast<const float*>(r);
+    const auto* tp = static_cast<const float*>(tau);
+    oracle::extrema_flags<float>(sh, std::vector<float>(rp, rp + sh.count), std::vector<float>(tp, tp + sh.count), f, ext);
+  } else {
+    const auto* rp = static_cast<const double*>(r);
+    const auto* tp = static_cast<const double*>(tau);
+    oracle::extrema_flags<double>(sh, std::vector<double>(rp, rp + sh.count), std::vector<double>(tp, tp + sh.count), f,
+                                  ext);
+  }
+  std::copy(f.begin(), f.end(), flags);
+  return 0;
+}
+
+int eda_oracle_components(int dim, const int64_t* n, const uint8_t* mask, int64_t* labels) {
+  const oracle::Shape sh(dim, n);
+  const std::vector<uint8_t> m(mask, mask + sh.count);
+  const std::vector<int64_t> lab = oracle::components(sh, m);
+  std::copy(lab.begin(), lab.end(), labels);
+  return 0;
+}
+
 int eda_oracle_cube(int dtype, int dim, const int64_t* n, int op, int32_t w, void* f) {
   const oracle::Shape sh(dim, n);
   const auto body = [&](auto tag) {

@@ -61,6 +61,13 @@ def lib() -> ctypes.CDLL:
         L.eda_oracle_rung_ladder.restype = ctypes.c_int
         L.eda_oracle_cube.argtypes = [ctypes.c_int, ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int32, ctypes.c_void_p]
         L.eda_oracle_cube.restype = ctypes.c_int
+        L.eda_oracle_select.argtypes = [f64p, ctypes.c_int64, ctypes.c_double, f64p]
+        L.eda_oracle_select.restype = ctypes.c_int
+        L.eda_oracle_flags.argtypes = [ctypes.c_int, ctypes.c_int, i64p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+        L.eda_oracle_flags.restype = ctypes.c_int
+        L.eda_oracle_components.argtypes = [ctypes.c_int, i64p, ctypes.c_void_p, i64p]
+        L.eda_oracle_components.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -159,6 +166,37 @@ def cube(f: np.ndarray, op: str, w: int) -> np.ndarray:
     code = {"max": 0, "min": 1, "box": 3}[op]
     lib().eda_oracle_cube(0 if f.dtype == np.float32 else 1, f.ndim, _p(n, ctypes.c_int64), code, w, f.ctypes.data)
     return f
+
+
+def select(values: np.ndarray, q: float = -1.0) -> float:
+    """The exact median (q < 0) or NumPy "linear" quantile of the doubles in values (NaN if empty)."""
+    v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    out = np.zeros(1, np.float64)
+    lib().eda_oracle_select(_p(v, ctypes.c_double), v.size, float(q), _p(out, ctypes.c_double))
+    return float(out[0])
+
+
+def flags(r: np.ndarray, tau: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The significant-extrema flags of one element r (*spatial) against the threshold field tau:
+    u8 flags (bit a: an extremum of a line along axis a) and the counts per axis."""
+    r = np.ascontiguousarray(r)
+    tau = np.ascontiguousarray(tau, dtype=r.dtype)
+    n = np.asarray(r.shape, dtype=np.int64)
+    out = np.zeros(r.shape, np.uint8)
+    ext = np.zeros(3, np.uint64)
+    lib().eda_oracle_flags(0 if r.dtype == np.float32 else 1, r.ndim, _p(n, ctypes.c_int64), r.ctypes.data,
+                           tau.ctypes.data, out.ctypes.data, _p(ext, ctypes.c_uint64))
+    return out, ext[:r.ndim].copy()
+
+
+def components(mask: np.ndarray) -> np.ndarray:
+    """Face-connected components of mask != 0 of one element: the smallest index of the sample's
+    component, -1 outside."""
+    m = np.ascontiguousarray(mask != 0, dtype=np.uint8)
+    n = np.asarray(m.shape, dtype=np.int64)
+    out = np.zeros(m.shape, np.int64)
+    lib().eda_oracle_components(m.ndim, _p(n, ctypes.c_int64), m.ctypes.data, _p(out, ctypes.c_int64))
+    return out
 
 
 def cores() -> int:
