@@ -2,6 +2,7 @@
 // The C ABI (include/eda_b200.h): exceptions become status codes and a per-thread message.
 #include "../../include/eda_b200.h"
 #include "driver.hpp"
+#include "orient.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -302,5 +303,14 @@ int eda_release_workspace(void) {
     edab::thread_staging().release();
   });
 }
+
+int eda_set_transform_precision(int mode) {
+  return guarded([&] {
+    if (mode < 0 || mode > 2) throw std::invalid_argument("eda: transform precision must be 0 (3xTF32), 1 (BF16x3) or 2 (FP32)");
+    edab::set_transform_precision(static_cast<edab::TransformPrecision>(mode));
+  });
+}
+
+int eda_transform_precision(void) { return static_cast<int>(edab::transform_precision()); }
 
 }  // extern "C"

@@ -7,6 +7,8 @@
 // (orient_tc.cu, 3xTF32); float64 passes run the SIMT product below (FP64 accumulation).
 #include "orient.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -404,6 +406,22 @@ float tf32_rna(float v) {
   return r;
 }
 
+// bfloat16 of a float32, round to nearest even (finite values), and back.
+uint16_t bf16_rne(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return static_cast<uint16_t>(u >> 16);
+}
+float bf16_float(uint16_t b) {
+  const uint32_t u = static_cast<uint32_t>(b) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+std::atomic<int> g_transform_precision{static_cast<int>(TransformPrecision::kTf32x3)};
+
 template <class T>
 void upload_axis(OrientPlan& p, int a, int32_t n) {
   // the bases in long double, rounded once to the dtype
@@ -452,10 +470,31 @@ void upload_axis(OrientPlan& p, int a, int32_t n) {
       EDAB_CUDA(cudaMalloc(dst, tb * sizeof(float)));
       EDAB_CUDA(cudaMemcpy(*dst, h.data(), tb * sizeof(float), cudaMemcpyHostToDevice));
     };
+    // the bfloat16 split: hi = bf16(v), lo = bf16(v - hi), round to nearest even
+    const auto split16 = [&](auto&& value, void** dst) {
+      std::vector<uint16_t> h(tb, 0);
+      for (int32_t j = 0; j < n; ++j) {
+        for (int32_t k = 0; k < n; ++k) {
+          const long double v = value(j, k);
+          const uint16_t hi = bf16_rne(static_cast<float>(v));
+          const uint16_t lo = bf16_rne(static_cast<float>(v - static_cast<long double>(bf16_float(hi))));
+          h[static_cast<size_t>(j) * kpad + k] = hi;
+          h[static_cast<size_t>(npad + j) * kpad + k] = lo;
+        }
+      }
+      EDAB_CUDA(cudaMalloc(dst, tb * sizeof(uint16_t)));
+      EDAB_CUDA(cudaMemcpy(*dst, h.data(), tb * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    };
     // forward: output frequency j, input sample k; inverse: output sample j, input frequency k
-    split([&](int32_t j, int32_t k) { return exact_c[static_cast<size_t>(j) * n + k]; }, &p.tc_fwd[a]);
-    split([&](int32_t j, int32_t k) { return exact_c[static_cast<size_t>(k) * n + j]; }, &p.tc_icos[a]);
-    split([&](int32_t j, int32_t k) { return exact_s[static_cast<size_t>(k) * n + j]; }, &p.tc_isin[a]);
+    const auto fwd_v = [&](int32_t j, int32_t k) { return exact_c[static_cast<size_t>(j) * n + k]; };
+    const auto icos_v = [&](int32_t j, int32_t k) { return exact_c[static_cast<size_t>(k) * n + j]; };
+    const auto isin_v = [&](int32_t j, int32_t k) { return exact_s[static_cast<size_t>(k) * n + j]; };
+    split(fwd_v, &p.tc_fwd[a]);
+    split(icos_v, &p.tc_icos[a]);
+    split(isin_v, &p.tc_isin[a]);
+    split16(fwd_v, &p.bf_fwd[a]);
+    split16(icos_v, &p.bf_icos[a]);
+    split16(isin_v, &p.bf_isin[a]);
   }
 }
 
@@ -499,8 +538,17 @@ void transform_axes(cudaStream_t s, const Geom& g, const OrientPlan& plan, const
     T* dst = step == D - 1 ? out : (src == buf0 ? buf1 : buf0);
     const int which = kinds[a];
     if constexpr (std::is_same_v<T, float>) {
-      const void* B = which == 0 ? plan.tc_fwd[a] : (which == 1 ? plan.tc_icos[a] : plan.tc_isin[a]);
-      rot_pass_tc(s, p, static_cast<const float*>(B), plan.kpad[a], plan.npad[a], src, dst, run, err);
+      const TransformPrecision mode = transform_precision();
+      if (mode == TransformPrecision::kFp32) {
+        const void* B = which == 0 ? plan.fwd[a] : (which == 1 ? plan.icos[a] : plan.isin[a]);
+        rot_pass_simt<T>(s, p, g.n[a], static_cast<const T*>(B), src, dst, run);
+      } else if (mode == TransformPrecision::kBf16x3) {
+        const void* B = which == 0 ? plan.bf_fwd[a] : (which == 1 ? plan.bf_icos[a] : plan.bf_isin[a]);
+        rot_pass_tc(s, p, B, true, plan.kpad[a], plan.npad[a], src, dst, run, err);
+      } else {
+        const void* B = which == 0 ? plan.tc_fwd[a] : (which == 1 ? plan.tc_icos[a] : plan.tc_isin[a]);
+        rot_pass_tc(s, p, B, false, plan.kpad[a], plan.npad[a], src, dst, run, err);
+      }
     } else {
       const void* B = which == 0 ? plan.fwd[a] : (which == 1 ? plan.icos[a] : plan.isin[a]);
       rot_pass_simt<T>(s, p, g.n[a], static_cast<const T*>(B), src, dst, run);
@@ -509,6 +557,13 @@ void transform_axes(cudaStream_t s, const Geom& g, const OrientPlan& plan, const
     src = dst;
   }
 }
+TransformPrecision transform_precision() {
+  return static_cast<TransformPrecision>(g_transform_precision.load(std::memory_order_relaxed));
+}
+void set_transform_precision(TransformPrecision p) {
+  g_transform_precision.store(static_cast<int>(p), std::memory_order_relaxed);
+}
+
 template void transform_axes<float>(cudaStream_t, const Geom&, const OrientPlan&, const float*, float*, float*,
                                     float*, const int*, const int32_t*, int32_t*);
 template void transform_axes<double>(cudaStream_t, const Geom&, const OrientPlan&, const double*, double*, double*,

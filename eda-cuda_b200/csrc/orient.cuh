@@ -29,9 +29,19 @@ struct OrientPlan {
   void* tc_fwd[kMaxDim] = {nullptr, nullptr, nullptr};
   void* tc_icos[kMaxDim] = {nullptr, nullptr, nullptr};
   void* tc_isin[kMaxDim] = {nullptr, nullptr, nullptr};
+  // the same split into bfloat16 hi and lo parts (BF16x3), [2][npad][kpad] bfloat16
+  void* bf_fwd[kMaxDim] = {nullptr, nullptr, nullptr};
+  void* bf_icos[kMaxDim] = {nullptr, nullptr, nullptr};
+  void* bf_isin[kMaxDim] = {nullptr, nullptr, nullptr};
   int32_t kpad[kMaxDim] = {0, 0, 0};
   int32_t npad[kMaxDim] = {0, 0, 0};
 };
+
+// The product of the float32 transforms (process-wide; float64 always runs the FP64 product):
+// 3xTF32 and BF16x3 split products on the tensor cores, or the plain float32 SIMT product.
+enum class TransformPrecision : int { kTf32x3 = 0, kBf16x3 = 1, kFp32 = 2 };
+TransformPrecision transform_precision();
+void set_transform_precision(TransformPrecision p);
 // The plan of a geometry and dtype on the current device (cached for the life of the process).
 const OrientPlan& orient_plan(const Geom& g, bool f64);
 // Samples of the orientation's work area: three ping-pong fields large enough for every rotated
@@ -48,10 +58,10 @@ struct RotPass {
   int32_t K;
   int64_t pitch_in, rows, f_in, n_lo, pitch_out, s_j, f_out;
 };
-// The pass on the tensor cores (float32, 3xTF32): basis [2][npad][kpad] hi / lo; *err set when a
-// bounded wait of the kernel expired.
-void rot_pass_tc(cudaStream_t s, const RotPass& p, const float* basis, int32_t kpad, int32_t npad, const float* in,
-                 float* out, const int32_t* run, int32_t* err);
+// The pass on the tensor cores (float32 data): basis [2][npad][kpad] hi / lo parts, float32 tf32
+// values (3xTF32) or bfloat16 (bf16: BF16x3); *err set when a bounded wait of the kernel expired.
+void rot_pass_tc(cudaStream_t s, const RotPass& p, const void* basis, bool bf16, int32_t kpad, int32_t npad,
+                 const float* in, float* out, const int32_t* run, int32_t* err);
 
 // The separable transform of every element with run[b] along all axes (last axis first), kinds[a]
 // = 0 forward DCT-II, 1 inverse cosine, 2 inverse sine basis on axis a: in (element layout) -> out

@@ -3,21 +3,24 @@
 // out = A B^T per element rows, A the field's rows along its contiguous axis (K = that axis),
 // B the n x n basis (forward DCT-II, inverse cosine or inverse sine) of that axis.
 //
-// Precision: 3xTF32. Each float32 operand x is split into hi = tf32(x) and lo = tf32(x - hi) (round
-// to nearest); the product is hi_a hi_b + hi_a lo_b + lo_a hi_b accumulated in float32 in tensor
-// memory (the dropped lo_a lo_b term is below 2^-22 of the product), so the transform keeps
-// float32-level accuracy (the reference runs these transforms with cuFFT in float32,
-// cpp/src/method/orientation.cu:674-767 of eda-cuda). The basis is split once on the host; the
-// field tile is split in shared memory after its TMA load.
+// Precision: split products with float32 accumulation in tensor memory, the float32 operand x split
+// into hi + lo and the product taken as hi_a hi_b + hi_a lo_b + lo_a hi_b (three MMAs; the dropped
+// lo_a lo_b term is below 2^-2p of the product). 3xTF32 (kind::tf32): hi = tf32(x), lo =
+// tf32(x - hi), about 22 bits of every operand; BF16x3 (kind::f16 on bfloat16): hi = bf16(x), lo =
+// bf16(x - hi), about 16 bits, at twice the MMA rate. (The reference runs these transforms with
+// cuFFT in float32, cpp/src/method/orientation.cu:674-767 of eda-cuda.) The basis is split once on
+// the host; the field tile is split in shared memory after its TMA load.
 //
 // Kernel (one 128 x 128 output tile per CTA, 192 threads):
 //   warp 4      TMA producer: A tile (128 rows x 32 floats, 128B swizzle) and the hi and lo basis
 //               tiles per k-block into a 3-stage ring (full / empty mbarriers);
-//   warps 0-3   split the A tile into hi (in place) and lo (second tile), fence the async proxy,
+//   warps 0-3   split the A tile into hi and lo tiles (3xTF32: hi in place, 128B swizzle; BF16x3:
+//               two bfloat16 tiles of 64-byte rows in the 64B swizzle), fence the async proxy,
 //               arrive on the stage's split barrier; then the epilogue: tcgen05.ld of their TMEM
 //               lane quarter and the transposed store;
-//   warp 5      allocates 128 TMEM columns; one thread issues 3 x 4 tcgen05.mma (kind::tf32,
-//               M = 128, N = 128, K = 8) per k-block and commits each stage back to the producer.
+//   warp 5      allocates 128 TMEM columns; one thread issues the split MMAs of every k-block
+//               (3 x 4 kind::tf32 with K = 8, or 3 x 2 kind::f16 with K = 16; M = N = 128) and
+//               commits each stage back to the producer.
 // The store writes the tile transposed: the transformed axis becomes the slowest axis of the
 // element and the next axis the contiguous one (a rotation of the layout), so every transform of
 // the orientation reads K-major rows, and D passes bring a field back to its layout.
@@ -34,17 +37,31 @@ namespace edab {
 namespace tc {
 
 constexpr int kBM = 128, kBN = 128, kBK = 32, kStages = 3;
-constexpr int kTileA = kBM * kBK * 4;  // 16 KiB
-constexpr int kTileB = kBN * kBK * 4;  // 16 KiB
-constexpr int kStageBytes = 2 * kTileA + 2 * kTileB;
-constexpr int kTmaBytes = kTileA + 2 * kTileB;  // A, B hi, B lo (the A lo tile is written by the split)
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
 constexpr int kThreadsTc = 192;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
-// Instruction descriptor of tcgen05.mma kind::tf32: D float32, A and B tf32, both K-major, N, M.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
-                            (static_cast<uint32_t>(kBM >> 4) << 24);
+// The stage layout of a split mode. 3xTF32: [A hi (TMA, then split in place) | A lo | B hi | B lo],
+// 16 KiB each, rows of 128 bytes. BF16x3: [A float32 (TMA) 16 KiB | A hi | A lo | B hi | B lo], the
+// bfloat16 tiles 8 KiB each, rows of 64 bytes. Every tile starts on a 1024-byte boundary.
+template <bool BF16>
+struct Stage {
+  static constexpr int kTileF32 = kBM * kBK * 4;                      // 16 KiB: the float32 A tile
+  static constexpr int kTileOp = BF16 ? kBM * kBK * 2 : kBM * kBK * 4;  // one operand tile
+  static constexpr int kAhi = BF16 ? kTileF32 : 0;
+  static constexpr int kAlo = kAhi + kTileOp;
+  static constexpr int kBhi = kAlo + kTileOp;
+  static constexpr int kBlo = kBhi + kTileOp;
+  static constexpr int kBytes = kBlo + kTileOp;
+  static constexpr int kTmaBytes = kTileF32 + 2 * kTileOp;  // A float32, B hi, B lo
+  static constexpr int kSmem = kStages * kBytes + 1024 + 256;
+};
+
+// Instruction descriptors (D float32, both operands K-major, N, M): kind::tf32 with tf32 A and B;
+// kind::f16 with bfloat16 A and B.
+constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
+                                (static_cast<uint32_t>(kBM >> 4) << 24);
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
+                                (static_cast<uint32_t>(kBM >> 4) << 24);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -55,6 +72,13 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
   return static_cast<uint64_t>((addr >> 4) & 0x3fffu) | (static_cast<uint64_t>(1) << 16) |
          (static_cast<uint64_t>(1024 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
          (static_cast<uint64_t>(2) << 61);
+}
+// The same for a K-major tile with the 64-byte swizzle: rows of 64 bytes, 8-row groups 512 bytes
+// apart, layout SWIZZLE_64B.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t addr) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3fffu) | (static_cast<uint64_t>(1) << 16) |
+         (static_cast<uint64_t>(512 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+         (static_cast<uint64_t>(4) << 61);
 }
 __device__ __forceinline__ unsigned long long now_ns() {
   unsigned long long t;
@@ -106,9 +130,24 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      "l"(adesc), "l"(bdesc), "r"(kIdescTf32), "r"(accumulate)
       : "memory");
 }
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdescBf16), "r"(accumulate)
+      : "memory");
+}
+// bfloat16 of x rounded to nearest even, as raw bits (x finite or infinite; NaN stays NaN).
+__device__ __forceinline__ uint32_t bf16_bits(float x) {
+  uint32_t r;
+  asm("{\n\t.reg .b16 h;\n\tcvt.rn.bf16.f32 h, %1;\n\tmov.b32 %0, {h, h};\n\t}" : "=r"(r) : "f"(x));
+  return r & 0xffffu;
+}
+__device__ __forceinline__ float bf16_value(uint32_t bits) { return __uint_as_float(bits << 16); }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
@@ -141,12 +180,14 @@ struct RotOut {
   int64_t f_out;      // output samples per element
 };
 
+template <bool BF16>
 __global__ void __launch_bounds__(kThreadsTc, 1)
     gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, RotOut ro,
             float* __restrict__ out, const int32_t* __restrict__ run, int32_t* __restrict__ err) {
+  using L = Stage<BF16>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * kStageBytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * L::kBytes);
   // bars: full[kStages], split[kStages], empty[kStages], acc
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * kStages + 1);
   __shared__ int32_t active_s;
@@ -192,12 +233,12 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           ok = false;
           break;
         }
-        unsigned char* st = base + s * kStageBytes;
+        unsigned char* st = base + s * L::kBytes;
         const uint32_t full = smem_u32(&bars[s]);
-        mbar_expect_tx(full, kTmaBytes);
+        mbar_expect_tx(full, L::kTmaBytes);
         tma_load_2d(smem_u32(st), &ta, kb * kBK, static_cast<int32_t>(m0), full);
-        tma_load_2d(smem_u32(st + 2 * kTileA), &tb, kb * kBK, n0, full);
-        tma_load_2d(smem_u32(st + 2 * kTileA + kTileB), &tb, kb * kBK, ro.npad + n0, full);
+        tma_load_2d(smem_u32(st + L::kBhi), &tb, kb * kBK, n0, full);
+        tma_load_2d(smem_u32(st + L::kBlo), &tb, kb * kBK, ro.npad + n0, full);
         issued = kb + 1;
       }
       // the copies of the last stages complete before the CTA may leave
@@ -215,16 +256,24 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a_hi = smem_u32(base + s * kStageBytes);
-        const uint32_t a_lo = a_hi + kTileA;
-        const uint32_t b_hi = a_hi + 2 * kTileA;
-        const uint32_t b_lo = b_hi + kTileB;
+        const uint32_t st = smem_u32(base + s * L::kBytes);
+        const uint32_t a_hi = st + L::kAhi, a_lo = st + L::kAlo, b_hi = st + L::kBhi, b_lo = st + L::kBlo;
+        if constexpr (BF16) {
 #pragma unroll
-        for (int kk = 0; kk < kBK / 8; ++kk) {
-          const uint32_t off = kk * 32;  // 8 tf32 of K inside the 128-byte swizzled row
-          mma_tf32(tmem, sw128_desc(a_hi + off), sw128_desc(b_hi + off), (kb | kk) != 0);
-          mma_tf32(tmem, sw128_desc(a_hi + off), sw128_desc(b_lo + off), 1u);
-          mma_tf32(tmem, sw128_desc(a_lo + off), sw128_desc(b_hi + off), 1u);
+          for (int kk = 0; kk < kBK / 16; ++kk) {
+            const uint32_t off = kk * 32;  // 16 bfloat16 of K inside the 64-byte swizzled row
+            mma_bf16(tmem, sw64_desc(a_hi + off), sw64_desc(b_hi + off), (kb | kk) != 0);
+            mma_bf16(tmem, sw64_desc(a_hi + off), sw64_desc(b_lo + off), 1u);
+            mma_bf16(tmem, sw64_desc(a_lo + off), sw64_desc(b_hi + off), 1u);
+          }
+        } else {
+#pragma unroll
+          for (int kk = 0; kk < kBK / 8; ++kk) {
+            const uint32_t off = kk * 32;  // 8 tf32 of K inside the 128-byte swizzled row
+            mma_tf32(tmem, sw128_desc(a_hi + off), sw128_desc(b_hi + off), (kb | kk) != 0);
+            mma_tf32(tmem, sw128_desc(a_hi + off), sw128_desc(b_lo + off), 1u);
+            mma_tf32(tmem, sw128_desc(a_lo + off), sw128_desc(b_hi + off), 1u);
+          }
         }
         mma_commit(smem_u32(&bars[2 * kStages + s]));
       }
@@ -240,23 +289,46 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         ok = false;
         break;
       }
-      float4* a = reinterpret_cast<float4*>(base + s * kStageBytes);
-      float4* alo = reinterpret_cast<float4*>(base + s * kStageBytes + kTileA);
+      unsigned char* st = base + s * L::kBytes;
+      float4* a = reinterpret_cast<float4*>(st);
+      if constexpr (BF16) {
+        // the float32 tile (128-byte rows, 16-byte unit u of row r at unit u ^ (r & 7)) into the hi
+        // and lo bfloat16 tiles (64-byte rows, 16-byte unit u of row r at unit u ^ ((r >> 1) & 3))
 #pragma unroll
-      for (int i = 0; i < kTileA / 16 / 128; ++i) {
-        const int idx = t + 128 * i;
-        const float4 v = a[idx];
-        float4 h, l;
-        h.x = to_tf32(v.x);
-        h.y = to_tf32(v.y);
-        h.z = to_tf32(v.z);
-        h.w = to_tf32(v.w);
-        l.x = to_tf32(__fsub_rn(v.x, h.x));
-        l.y = to_tf32(__fsub_rn(v.y, h.y));
-        l.z = to_tf32(__fsub_rn(v.z, h.z));
-        l.w = to_tf32(__fsub_rn(v.w, h.w));
-        a[idx] = h;
-        alo[idx] = l;
+        for (int i = 0; i < L::kTileF32 / 16 / 128; ++i) {
+          const int idx = t + 128 * i;  // the physical float4 of the float32 tile
+          const int r = idx >> 3;
+          const int k0 = ((idx & 7) ^ (r & 7)) * 4;  // its first K column
+          const float4 v = a[idx];
+          const float f[4] = {v.x, v.y, v.z, v.w};
+          uint32_t hb[4], lb[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            hb[q] = bf16_bits(f[q]);
+            lb[q] = bf16_bits(__fsub_rn(f[q], bf16_value(hb[q])));
+          }
+          const int at = r * 64 + ((((k0 >> 3) ^ ((r >> 1) & 3))) << 4) + ((k0 & 7) << 1);
+          *reinterpret_cast<uint2*>(st + L::kAhi + at) = make_uint2(hb[0] | (hb[1] << 16), hb[2] | (hb[3] << 16));
+          *reinterpret_cast<uint2*>(st + L::kAlo + at) = make_uint2(lb[0] | (lb[1] << 16), lb[2] | (lb[3] << 16));
+        }
+      } else {
+        float4* alo = reinterpret_cast<float4*>(st + L::kAlo);
+#pragma unroll
+        for (int i = 0; i < L::kTileF32 / 16 / 128; ++i) {
+          const int idx = t + 128 * i;
+          const float4 v = a[idx];
+          float4 h, l;
+          h.x = to_tf32(v.x);
+          h.y = to_tf32(v.y);
+          h.z = to_tf32(v.z);
+          h.w = to_tf32(v.w);
+          l.x = to_tf32(__fsub_rn(v.x, h.x));
+          l.y = to_tf32(__fsub_rn(v.y, h.y));
+          l.z = to_tf32(__fsub_rn(v.z, h.z));
+          l.w = to_tf32(__fsub_rn(v.w, h.w));
+          a[idx] = h;
+          alo[idx] = l;
+        }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(smem_u32(&bars[kStages + s]));
@@ -319,17 +391,19 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-// A 2-D float32 tensor map: inner extent `inner` (contiguous), `outer` rows `stride` floats apart,
-// boxes of 32 x box_rows with the 128-byte swizzle; reads past the extents return zeros.
-CUtensorMap make_map(const float* base, uint64_t inner, uint64_t outer, uint64_t stride, uint32_t box_rows) {
+// A 2-D tensor map of float32 (128-byte swizzle) or bfloat16 (64-byte swizzle) elements: inner
+// extent `inner` (contiguous), `outer` rows `stride` elements apart, boxes of 32 x box_rows
+// elements (one swizzled row each); reads past the extents return zeros.
+CUtensorMap make_map(const void* base, bool bf16, uint64_t inner, uint64_t outer, uint64_t stride, uint32_t box_rows) {
   CUtensorMap m;
   std::memset(&m, 0, sizeof m);
   const cuuint64_t dims[2] = {inner, outer};
-  const cuuint64_t strides[1] = {stride * sizeof(float)};
+  const cuuint64_t strides[1] = {stride * (bf16 ? 2 : 4)};
   const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), box_rows};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
-                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+  const CUresult r = encode_fn()(&m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                                 const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 bf16 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     throw CudaError("eda: cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")",
@@ -338,28 +412,22 @@ CUtensorMap make_map(const float* base, uint64_t inner, uint64_t outer, uint64_t
   return m;
 }
 
+template <bool BF16>
 void set_smem_once() {
-  static std::mutex mu;
-  static bool done[64] = {};
-  int dev = 0;
-  EDAB_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(mu);
-  if (!done[dev]) {
-    EDAB_CUDA(cudaFuncSetAttribute(gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    done[dev] = true;
+  if (first_on_device(reinterpret_cast<const void*>(gemm_tc<BF16>))) {
+    EDAB_CUDA(cudaFuncSetAttribute(gemm_tc<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, Stage<BF16>::kSmem));
   }
 }
 
 }  // namespace tc
 
 // One rotated axis pass on the tensor cores (orient.cuh): see RotPass.
-void rot_pass_tc(cudaStream_t s, const RotPass& p, const float* basis, int32_t kpad, int32_t npad, const float* in,
-                 float* out, const int32_t* run, int32_t* err) {
+void rot_pass_tc(cudaStream_t s, const RotPass& p, const void* basis, bool bf16, int32_t kpad, int32_t npad,
+                 const float* in, float* out, const int32_t* run, int32_t* err) {
   if (p.M < 1) return;
-  tc::set_smem_once();
-  const CUtensorMap ta = tc::make_map(in, static_cast<uint64_t>(p.K), static_cast<uint64_t>(p.M),
+  const CUtensorMap ta = tc::make_map(in, false, static_cast<uint64_t>(p.K), static_cast<uint64_t>(p.M),
                                       static_cast<uint64_t>(p.pitch_in), tc::kBM);
-  const CUtensorMap tb = tc::make_map(basis, static_cast<uint64_t>(kpad), static_cast<uint64_t>(2 * npad),
+  const CUtensorMap tb = tc::make_map(basis, bf16, static_cast<uint64_t>(kpad), static_cast<uint64_t>(2 * npad),
                                       static_cast<uint64_t>(kpad), tc::kBN);
   tc::RotOut ro{};
   ro.M = p.M;
@@ -374,7 +442,13 @@ void rot_pass_tc(cudaStream_t s, const RotPass& p, const float* basis, int32_t k
   const int64_t mt = (p.M + tc::kBM - 1) / tc::kBM;
   if (mt > 0x7fffffffLL) throw std::invalid_argument("eda: orientation pass too large");
   const dim3 grid(static_cast<unsigned>((p.K + tc::kBN - 1) / tc::kBN), static_cast<unsigned>(mt));
-  tc::gemm_tc<<<grid, tc::kThreadsTc, tc::kSmemBytes, s>>>(ta, tb, ro, out, run, err);
+  if (bf16) {
+    tc::set_smem_once<true>();
+    tc::gemm_tc<true><<<grid, tc::kThreadsTc, tc::Stage<true>::kSmem, s>>>(ta, tb, ro, out, run, err);
+  } else {
+    tc::set_smem_once<false>();
+    tc::gemm_tc<false><<<grid, tc::kThreadsTc, tc::Stage<false>::kSmem, s>>>(ta, tb, ro, out, run, err);
+  }
   EDAB_LAUNCH("gemm_tc");
 }
 

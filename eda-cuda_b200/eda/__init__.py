@@ -30,7 +30,28 @@ __all__ = [
     "device_count",
     "device_info",
     "monogenic",
+    "set_transform_precision",
+    "transform_precision",
 ]
+
+#: The products of the float32 orientation transforms (2-D / 3-D): split products on the tensor
+#: cores ("tf32x3", the default; "bf16x3") or the plain float32 product ("fp32").
+TRANSFORM_PRECISIONS = ("tf32x3", "bf16x3", "fp32")
+
+
+def set_transform_precision(name: str) -> None:
+    """Selects the product of the float32 orientation transforms for the whole process: "tf32x3"
+    (3xTF32 split products on the tensor cores, the default), "bf16x3" (BF16x3 split products on
+    the tensor cores) or "fp32" (the plain float32 product). Float64 input always uses float64. This
+    engine's extension: the reference computes the transforms with cuFFT in float32."""
+    if name not in TRANSFORM_PRECISIONS:
+        raise ValueError(f"eda: transform precision must be one of {TRANSFORM_PRECISIONS}, got {name!r}")
+    _native.core().set_transform_precision(TRANSFORM_PRECISIONS.index(name))
+
+
+def transform_precision() -> str:
+    """The current product of the float32 orientation transforms (see set_transform_precision)."""
+    return TRANSFORM_PRECISIONS[_native.core().transform_precision()]
 
 
 def build_info() -> dict[str, Any]:

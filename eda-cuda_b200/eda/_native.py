@@ -77,8 +77,17 @@ class Core:
                                     ctypes.c_int, ctypes.POINTER(i32), vp]
         L.eda_ragged_free.argtypes = [vp]
         L.eda_ragged_free.restype = None
+        L.eda_set_transform_precision.argtypes = [ctypes.c_int]
+        L.eda_transform_precision.argtypes = []
         self._lib = L
         self.path = str(path)
+
+    # -- the float32 transforms' product ------------------------------------------------------
+    def set_transform_precision(self, mode: int) -> None:
+        self._check(self._lib.eda_set_transform_precision(int(mode)))
+
+    def transform_precision(self) -> int:
+        return int(self._lib.eda_transform_precision())
 
     # -- errors --------------------------------------------------------------------------------
     def _check(self, status: int) -> None:

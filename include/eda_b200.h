@@ -175,6 +175,15 @@ EDA_API int eda_device_info(int device, char* buf, size_t len);
  * (the reference's Context::release_unused_memory, cpp/src/runtime/context.cpp:154-160). */
 EDA_API int eda_release_workspace(void);
 
+/* The product of the float32 orientation transforms, process-wide (no counterpart in the reference,
+ * whose transforms are cuFFT's float32 FFTs, cpp/src/method/orientation.cu:674-767): 0 = 3xTF32
+ * split products on the tensor cores (the default), 1 = BF16x3 split products on the tensor cores,
+ * 2 = the plain float32 SIMT product. Float64 fields always use the float64 product. Changing it
+ * between calls changes float32 2-D / 3-D results within the transforms' precision (about 1e-6 of
+ * the field for 3xTF32 and FP32, 1e-5 for BF16x3). eda_transform_precision returns the current one. */
+EDA_API int eda_set_transform_precision(int mode);
+EDA_API int eda_transform_precision(void);
+
 /* The allocation-free decomposition (no counterpart in the reference), for callers that must not
  * allocate device memory: plugin hosts whose device allocator belongs to the host application, and
  * real-time loops that forbid allocation after start-up. It computes what eda_decompose computes,

@@ -222,3 +222,36 @@ def test_transform_matches_the_bases_in_float64(dev, shape, kinds, dtype):
     err = np.max(np.abs(got - want))
     tol = (2e-5 if dtype == np.float32 else 1e-12) * np.max(np.abs(want))
     assert err <= tol, (shape, kinds, err, tol)
+
+
+# the float32 transforms' products: their error against the float64 bases (relative to the
+# result's largest magnitude) in every mode; the mode is process-wide, restored afterwards
+PRECISION_TOL = {0: 2e-5, 1: 2e-4, 2: 2e-5}
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("shape,kinds", TRANSFORMS, ids=["x".join(map(str, s)) + "-" + "".join(map(str, k))
+                                                          for s, k in TRANSFORMS])
+def test_transform_precision_arms(dev, shape, kinds, mode):
+    torch, lib = dev
+    lib.eda_set_transform_precision.argtypes = [ctypes.c_int]
+    lib.eda_transform_precision.restype = ctypes.c_int
+    rng = np.random.default_rng(len(shape) * 100 + shape[0] + mode)
+    x = rng.standard_normal((3,) + shape).astype(np.float32)
+    assert lib.eda_set_transform_precision(mode) == 0
+    try:
+        assert lib.eda_transform_precision() == mode
+        got = gpu_transform(dev, x, kinds)
+    finally:
+        lib.eda_set_transform_precision(0)
+    want = host_transform(x, kinds)
+    err = np.max(np.abs(got - want))
+    tol = PRECISION_TOL[mode] * np.max(np.abs(want))
+    assert err <= tol, (shape, kinds, mode, err, tol)
+
+
+def test_transform_precision_rejects_unknown_modes(dev):
+    torch, lib = dev
+    lib.eda_set_transform_precision.argtypes = [ctypes.c_int]
+    assert lib.eda_set_transform_precision(3) == 1
+    assert lib.eda_set_transform_precision(-1) == 1
