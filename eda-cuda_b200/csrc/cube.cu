@@ -103,8 +103,9 @@ __device__ __forceinline__ T fold_identity() {
 struct Win {
   int32_t r, wa, o, k_lo, nseg, cps;
 };
-// 32-bit arithmetic throughout (n <= 8192 and wa <= 2n - 1, so n (wa + 1) / 2 < 2^27): the 64-bit
-// integer divisions of a general formula are long emulated sequences on the GPU.
+// 32-bit arithmetic but for the offset's product (n (wa + 1) / 2 reaches 2^32 for the longest
+// lines; one 64-bit modulo per window set-up): the 64-bit integer divisions of a general formula
+// are long emulated sequences on the GPU.
 __device__ __forceinline__ int32_t floor_div32(int32_t a, int32_t b) {  // b > 0
   const int32_t q = a / b;
   return (a % b != 0 && a < 0) ? q - 1 : q;
@@ -114,8 +115,8 @@ __device__ __forceinline__ Win make_win(int32_t n, int32_t w) {
   const int32_t half = (w - 1) >> 1;
   q.r = min(half, n - 1);
   q.wa = 2 * q.r + 1;
-  q.o = static_cast<int32_t>((static_cast<uint32_t>(n) * static_cast<uint32_t>((q.wa + 1) >> 1)) %
-                             static_cast<uint32_t>(q.wa));
+  q.o = static_cast<int32_t>((static_cast<uint64_t>(n) * static_cast<uint64_t>((q.wa + 1) >> 1)) %
+                             static_cast<uint64_t>(q.wa));
   q.k_lo = floor_div32(q.r - q.o, q.wa);
   const int32_t k_hi = floor_div32(n - 1 + q.r - q.o, q.wa);
   q.nseg = k_hi - q.k_lo + 1;
@@ -335,6 +336,19 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   const T* Vp = V + p * LS;
   T* Rp = R + p * LS;
   const T idn = fold_identity<T, OP>();
+  if (q.wa == 1) {
+    // one-sample segments: H = G = the sample, so y = op(v, v): the sample for max / min, and for
+    // sums the aligned mean (v + v) * 0.5 of the canonical path, rounded the same way
+    for (int32_t i = worker; i < n; i += workers) {
+      const T v = Vp[i * PP];
+      Rp[i * PP] = OP == kOpSum ? mul_rn(add_rn(v, v), T(0.5)) : v;
+    }
+    __syncthreads();
+    return;
+  }
+  // segments of one chunk (wa <= 32) run in runs of `per` consecutive segments, one run per task
+  // (about one task per worker): a task's set-up is paid once per run, not once per segment
+  const int32_t per = q.cps == 1 ? (q.nseg + workers - 1) / workers : 1;
   if (q.cps > 1) {
     // phase 1: chunk totals; half of the workers take the line, half the reversed line
     constexpr int half = workers / 2;
@@ -378,6 +392,20 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     __syncthreads();
   }
   // phase 3: H (the reversed line's G) into R at the output slots n - 1 + r - e (e >= r)
+  if (per > 1) {
+    const int32_t k_end = min((worker + 1) * per, q.nseg);
+    for (int32_t k = worker * per; k < k_end; ++k) {
+      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+      const int32_t c1 = min(s + q.wa - 1, e_max);
+      if (s >= 0 && c1 <= n - 1) {
+        partial_h<T, OP, PP>(Vp + (n - 1 - s) * PP, Rp + (n - 1 + q.r - s) * PP, c1 - s + 1, max(0, q.r - s), idn);
+      } else {
+        fold_chunk<T, OP>(Vp, PP, n, s, c1, 1, [&](int32_t e, T loc) {
+          if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = fop<OP>(idn, loc);
+        });
+      }
+    }
+  } else
   for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
     const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
@@ -398,6 +426,30 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   }
   __syncthreads();
   // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r)), slot x = e - r
+  if (per > 1) {
+    const int32_t k_end = min((worker + 1) * per, q.nseg);
+    for (int32_t k = worker * per; k < k_end; ++k) {
+      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+      const int32_t e_al = s + q.wa - 1;
+      const int32_t c1 = min(e_al, e_max);
+      if (s >= 0 && c1 <= n - 1) {
+        partial_g<T, OP, PP>(Vp + s * PP, Rp + (s - q.r) * PP, c1 - s + 1, max(0, q.r - s), idn, c1 == e_al);
+      } else {
+        fold_chunk<T, OP>(Vp, PP, n, s, c1, 0, [&](int32_t e, T loc) {
+          if (e < q.r) return;
+          const T g = fop<OP>(idn, loc);
+          T* slot = Rp + (e - q.r) * PP;
+          const T h = *slot;
+          if constexpr (OP == kOpSum) {
+            const T sum = add_rn(h, g);
+            *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+          } else {
+            *slot = fop<OP>(h, g);
+          }
+        });
+      }
+    }
+  } else
   for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
     const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
     const int32_t e_al = s + q.wa - 1;
@@ -770,6 +822,82 @@ __global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) 
   if (a.bytes && threadIdx.x == 0 && acct) atomicAdd(a.bytes, acct);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Lines too long to stage in shared memory (1-D signals beyond the staged capacity; the other
+// axes stay within it). The line's fold input (order keys for max / min, the samples or the
+// bit field's 0 / 1 for sums) is written once per element into a global scratch; then one CTA per
+// element and rung runs the same fold phases as the staged kernel with P = 1 on global memory (the
+// line and its outputs stay in L2), the chunk totals in shared memory, and the output line in the
+// rung's output field, finished in place by the pass's epilogue. The canonical folds, and so every
+// bit of the result, are those of the staged kernel.
+template <class T>
+__global__ void __launch_bounds__(kThreads) long_line_input(Geom g, PassArgs<T> a, T* keys) {
+  const int64_t total = g.batch * g.pitch;  // 1-D: one row per element
+  const bool box = a.op == static_cast<int>(CubeOp::kBox);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    T v;
+    if (a.bits) v = ((a.bits[i] >> a.bit) & 1u) ? T(1) : T(0);
+    else v = a.in0[i];
+    keys[i] = box ? v : okey(v);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) cube_long(Geom g, PassArgs<T> a, const T* __restrict__ keys) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ Win q_s;
+  __shared__ T fac_s;
+  const int64_t b = blockIdx.x;
+  const int32_t j = static_cast<int32_t>(blockIdx.y);
+  const int32_t n = g.n_last;
+  const int32_t w = a.win[static_cast<int64_t>(j) * g.batch + b];
+  if (w < 1) return;
+  const bool box = a.op == static_cast<int>(CubeOp::kBox);
+  if (threadIdx.x == 0) {
+    q_s = make_win(n, w);
+    if (box && a.last) fac_s = static_cast<T>(1.0 / static_cast<double>(2 * min((w - 1) / 2, n - 1) + 1));
+  }
+  __syncthreads();
+  const Win q = q_s;
+  const int32_t TS = tot_slots(n);
+  T* tot = reinterpret_cast<T*>(smem_raw);
+  const T* V = keys + b * g.pitch;
+  const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
+  const bool detsq = box && a.last && a.epi == static_cast<int>(BoxEpi::kDetSq);
+  for (int f = 0; f < nf; ++f) {
+    T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
+    const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
+    if (box) run_stage<T, kOpSum, 1, 1>(V, R, tot, n, TS, q, 0);
+    else if (is_min) run_stage<T, kOpMinK, 1, 1>(V, R, tot, n, TS, q, 0);
+    else run_stage<T, kOpMaxK, 1, 1>(V, R, tot, n, TS, q, 0);
+    // the epilogue in place (run_stage ended on a barrier: every output is written); pads are 0
+    const T* aux = detsq ? a.aux + b * g.field : nullptr;
+    for (int32_t i = threadIdx.x; i < static_cast<int32_t>(g.pitch); i += blockDim.x) {
+      T y = i < n ? R[i] : T(0);
+      if (i < n) {
+        if (!box) {
+          y = okey(y);
+        } else if (a.last) {
+          y = mul_rn(y, fac_s);
+          if (detsq) {
+            const T d = sub_rn(aux[i], y);
+            y = mul_rn(d, d);
+          }
+        }
+      }
+      R[i] = y;
+    }
+    __syncthreads();
+  }
+  if (a.bytes && threadIdx.x == 0) {
+    atomicAdd(a.bytes, static_cast<unsigned long long>(n) * sizeof(T) * (1 + nf));
+  }
+}
+
+thread_local void* t_long_scratch = nullptr;
+thread_local size_t t_long_bytes = 0;
+
 size_t smem_bytes(int32_t n, int P, bool rows, size_t es) {
   const int32_t gel = es == 4 ? group_elems<float>(n, P, rows) : group_elems<double>(n, P, rows);
   return (static_cast<size_t>(3) * gel + static_cast<size_t>(2) * tot_slots(n) * P) * es;
@@ -834,9 +962,37 @@ int lines_per_cta(const Geom& g, int axis, size_t cap) {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 template <class T>
+void launch_long(cudaStream_t s, const Geom& g, PassArgs<T> a) {
+  if (g.dim != 1) throw std::invalid_argument("edab: lines beyond the shared-memory capacity are 1-D only");
+  const size_t need = static_cast<size_t>(g.batch) * static_cast<size_t>(g.pitch) * sizeof(T);
+  if (t_long_scratch == nullptr || t_long_bytes < need) {
+    throw std::logic_error("edab: a long-line cube pass needs the thread's long-line scratch");
+  }
+  T* keys = static_cast<T*>(t_long_scratch);
+  long_line_input<T><<<blocks_for(g.batch * g.pitch), kThreads, 0, s>>>(g, a, keys);
+  EDAB_LAUNCH("long_line_input");
+  const size_t smem = static_cast<size_t>(2) * tot_slots(g.n_last) * sizeof(T);
+  if (first_on_device(reinterpret_cast<const void*>(cube_long<T>))) {
+    EDAB_CUDA(cudaFuncSetAttribute(cube_long<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(dev_facts().smem)));
+  }
+  if (smem > dev_facts().smem) throw std::invalid_argument("edab: a line is too long for the long-line cube pass");
+  if (g.batch > 0x7fffffffLL || a.rungs > 65535) throw std::invalid_argument("edab: cube launch too large");
+  a.bytes = cube_bytes_counter();
+  profile_cube_launch(s, true);
+  cube_long<T><<<dim3(static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs)), kThreads, smem, s>>>(g, a, keys);
+  EDAB_LAUNCH("cube_long");
+  profile_cube_launch(s, false);
+}
+
+template <class T>
 void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   const DevFacts f = dev_facts();
   const bool rows = a.axis == g.dim - 1;
+  if (rows && smem_bytes(g.n[a.axis], 1, true, sizeof(T)) > f.smem) {
+    launch_long<T>(s, g, a);
+    return;
+  }
   const int P = lines_per_cta<T>(g, a.axis, f.smem);
   if (a.rungs > kMaxRungs) throw std::invalid_argument("edab: more rungs than a cube launch holds");
   int64_t groups;
@@ -943,6 +1099,18 @@ void cube(cudaStream_t s, const Geom& g, CubeOp op, const CubeArgs<T>& c) {
     a.out1 = c.out1;
     launch_pass<T>(s, g, a);
   }
+}
+
+void set_long_line_scratch(void* p, size_t bytes) {
+  t_long_scratch = p;
+  t_long_bytes = bytes;
+}
+
+size_t long_line_scratch_bytes(const Geom& g, size_t es) {
+  if (g.dim != 1) return 0;
+  const size_t staged = es == 4 ? smem_bytes(g.n_last, 1, true, 4) : smem_bytes(g.n_last, 1, true, 8);
+  if (staged <= dev_facts().smem) return 0;
+  return static_cast<size_t>(g.batch) * static_cast<size_t>(g.pitch) * es;
 }
 
 template <class T>

@@ -209,8 +209,12 @@ __global__ void orient_collect_kernel(int64_t B, int32_t D, int64_t count, int32
   }
 }
 
-// The longest axis: a cube pass stages whole lines in shared memory (the reference's limits).
-int32_t max_axis(int dtype) { return dtype == 0 ? 8192 : 4096; }
+// The longest axis. 2-D and 3-D: the reference's limits (8192 float32, 4096 float64 samples; the
+// passes stage whole lines in shared memory). 1-D signals: up to kMaxLine1D samples in either
+// dtype (the reference stops at the 2-D limits); lines beyond the staged capacity fold in global
+// memory (cube.cu, stats.cu).
+constexpr int32_t kMaxLine1D = 65536;
+int32_t max_axis(int dtype, int dim) { return dim == 1 ? kMaxLine1D : (dtype == 0 ? 8192 : 4096); }
 
 }  // namespace
 
@@ -313,7 +317,7 @@ void Run::collect_one(int64_t j, void* dst, bool dst_on_device, cudaStream_t s) 
 void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params& p) {
   if (dim < 1 || dim > kMaxDim) throw std::invalid_argument("eda: D must be 1, 2 or 3");
   if (dtype != 0 && dtype != 1) throw std::invalid_argument("eda: the input must be float32 or float64");
-  const int32_t lim = max_axis(dtype);
+  const int32_t lim = max_axis(dtype, dim);
   for (int a = 0; a < dim; ++a) {
     if (n[a] < 1) throw std::invalid_argument("eda: every spatial extent must be >= 1");
     if (n[a] > lim) {

@@ -382,6 +382,11 @@ template <class T>
 void cube(cudaStream_t s, const Geom& g, CubeOp op, const CubeArgs<T>& a);
 template <class T>
 void cube_simple(cudaStream_t s, const Geom& g, CubeOp op, const T* in, T* out0, T* out1, const int32_t* win);
+// 1-D lines too long for a pass to stage in shared memory fold in global memory: the calling host
+// thread provides a scratch of long_line_scratch_bytes (batch x pitch samples; 0 when the lines
+// fit) for the lines' fold input, before its cube calls.
+size_t long_line_scratch_bytes(const Geom& g, size_t es);
+void set_long_line_scratch(void* p, size_t bytes);
 
 // Canonical reductions: per element sum v^2 (canonical tree) and max|v| of f.
 template <class T>

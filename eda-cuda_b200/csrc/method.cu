@@ -1626,15 +1626,26 @@ size_t engine_bytes(const Geom& g) {
   if (D >= 2) b += static_cast<size_t>(orient_work_samples(g)) * sizeof(T);
   b += static_cast<size_t>(g.batch) * (sizeof(Elem) + 4 * (kSlots + kMasks + kMaxRungs) + 8 * 10 + 64);
   b += select_scratch_bytes(g) + totals_scratch_bytes(g);
+  b += long_line_scratch_bytes(g, sizeof(T));  // 1-D lines beyond the cube passes' staged capacity
   b += 160 * 256;  // every take is rounded up to 256 bytes
   return b;
 }
+
+namespace {
+// The long-line scratch of the calling thread for the duration of one engine run.
+struct LongLineScratch {
+  LongLineScratch(void* p, size_t bytes) { set_long_line_scratch(p, bytes); }
+  ~LongLineScratch() { set_long_line_scratch(nullptr, 0); }
+};
+}  // namespace
 
 template <class T>
 void run_chunk(const Geom& g, const Ctl& c, cudaStream_t s, Workspace& ws, const T* x, T* rows, int32_t* hs,
                int32_t* hf, double* hp, double* he, std::vector<Elem>& out, T* orient) {
   Engine<T> e(g, c, s, ws);
   e.orient_out_ = g.dim >= 2 ? orient : nullptr;
+  const size_t lb = long_line_scratch_bytes(g, sizeof(T));
+  const LongLineScratch scratch(lb ? ws.take<unsigned char>(lb) : nullptr, lb);
   e.run(x, rows, hs, hf, hp, he, out);
 }
 

@@ -135,6 +135,15 @@ void monogenic(const void* x, bool on_device, int dtype, int dim, int64_t batch,
                void* out, bool out_on_device, int32_t* nonfinite, cudaStream_t s) {
   Params p;
   validate(dtype, dim, batch, n, p);
+  // the monogenic transforms are dense products with n x n bases: every axis stays within the
+  // 2-D / 3-D limits (the reference's), also in 1-D
+  const int64_t lim = dtype == 0 ? 8192 : 4096;
+  for (int a = 0; a < dim; ++a) {
+    if (n[a] > lim) {
+      throw std::invalid_argument("eda: axis extent " + std::to_string(n[a]) + " exceeds the limit " + std::to_string(lim) +
+                                  (dtype == 0 ? " for float32" : " for float64"));
+    }
+  }
   if (max_chunk < 0) throw std::invalid_argument("eda: max_chunk must be >= 0");
   int64_t count = 1;
   for (int a = 0; a < dim; ++a) count *= n[a];

@@ -513,10 +513,10 @@ __device__ __forceinline__ T xs(const T* x, int32_t k) {
 // Samples k = from, from + Dir, .. to of a staged line against the peak value v: 1 when a sample
 // lies a significant drop away from v before any sample lies beyond v (above a maximum, below a
 // minimum, or NaN), 0 when a sample beyond v comes first, -1 when the range holds neither.
-template <bool Max, int Dir, class T>
-__device__ __forceinline__ int walk_samples(const T* x, int32_t from, int32_t to, T v, T tau) {
+template <bool Max, int Dir, class T, class X>
+__device__ __forceinline__ int walk_samples(const X& x, int32_t from, int32_t to, T v, T tau) {
   for (int32_t k = from; (to - k) * Dir >= 0; k += Dir) {
-    const T u = xs(x, k);
+    const T u = x(k);
     if (Max ? !(u <= v) : !(u >= v)) return 0;
     if (Max ? drops(v, u, tau) : drops(u, v, tau)) return 1;
   }
@@ -529,20 +529,20 @@ __device__ __forceinline__ int walk_samples(const T* x, int32_t from, int32_t to
 // judged by its extremes (bext: the extreme towards "beyond", bnear: the other one): a block with
 // nothing beyond v either holds a significant drop or is passed over; the first block with a sample
 // beyond v is walked and decides.
-template <bool Max, int Dir, class T>
-__device__ bool side_falls(const T* x, int32_t n, int32_t p, T v, T tau, const T* bext, const T* bnear) {
+template <bool Max, int Dir, class T, class X>
+__device__ bool side_falls(const X& x, int32_t n, int32_t p, T v, T tau, const T* bext, const T* bnear) {
   const int32_t blocks = (n + kBlk - 1) / kBlk;
   int32_t c = p / kBlk;
   const int32_t edge = Dir > 0 ? min(c * kBlk + kBlk - 1, n - 1) : c * kBlk;
   if ((edge - p) * Dir > 0) {
-    const int verdict = walk_samples<Max, Dir>(x, p + Dir, edge, v, tau);
+    const int verdict = walk_samples<Max, Dir, T>(x, p + Dir, edge, v, tau);
     if (verdict >= 0) return verdict == 1;
   }
   for (c += Dir; c >= 0 && c < blocks; c += Dir) {
     const T e = bext[c];
     if (Max ? !(e <= v) : !(e >= v)) {
       const int32_t first = c * kBlk, last = min(first + kBlk - 1, n - 1);
-      return walk_samples<Max, Dir>(x, Dir > 0 ? first : last, Dir > 0 ? last : first, v, tau) == 1;
+      return walk_samples<Max, Dir, T>(x, Dir > 0 ? first : last, Dir > 0 ? last : first, v, tau) == 1;
     }
     if (Max ? drops(v, bnear[c], tau) : drops(bnear[c], v, tau)) return true;
   }
@@ -664,8 +664,9 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
     const int32_t pk = (s + e) / 2;
     const int64_t at = eoff + base_s[p] + pk * step;
     const T tp = pk == s ? tp_s : tau[at];
-    const bool sig = is_max ? side_falls<true, -1>(x, n, pk, cur, tp, pmax, pmin) && side_falls<true, 1>(x, n, pk, cur, tp, pmax, pmin)
-                            : side_falls<false, -1>(x, n, pk, cur, tp, pmin, pmax) && side_falls<false, 1>(x, n, pk, cur, tp, pmin, pmax);
+    const auto at_k = [x](int32_t k) { return xs(x, k); };
+    const bool sig = is_max ? side_falls<true, -1>(at_k, n, pk, cur, tp, pmax, pmin) && side_falls<true, 1>(at_k, n, pk, cur, tp, pmax, pmin)
+                            : side_falls<false, -1>(at_k, n, pk, cur, tp, pmin, pmax) && side_falls<false, 1>(at_k, n, pk, cur, tp, pmin, pmax);
     if (sig) {
       flags[at] |= static_cast<uint8_t>(1u << axis);
       ++mine;
@@ -690,6 +691,83 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   __syncthreads();
   if (threadIdx.x == 0 && count_s) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&el[b].ext[axis]), static_cast<unsigned long long>(count_s));
+  }
+}
+
+// Lines too long to stage (1-D signals beyond the staged capacity): one CTA per line reads the
+// samples from global memory (L1 / L2) and keeps only the 32-sample block extremes in shared
+// memory; the peaks and their walks are those of the staged kernel.
+template <class T>
+__global__ void __launch_bounds__(kThreads) flags_long(Geom g, const T* __restrict__ r, const T* __restrict__ tau,
+                                                       uint8_t* __restrict__ flags, Elem* el, const int32_t* run) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int32_t count_s;
+  const int64_t b = blockIdx.y;
+  if (run && !run[b]) return;
+  const int64_t row = blockIdx.x;
+  const int32_t n = g.n_last;
+  const int32_t nb = (n + kBlk - 1) / kBlk;
+  T* bmin = reinterpret_cast<T*>(smem_raw);
+  T* bmax = bmin + nb;
+  const int64_t base = b * g.field + row * g.pitch;
+  const T* line = r + base;
+  if (threadIdx.x == 0) count_s = 0;
+  for (int32_t c = threadIdx.x; c < nb; c += blockDim.x) {
+    const int32_t len = min(kBlk, n - c * kBlk);
+    const T* xb = line + c * kBlk;
+    T mn = xb[0], mx = mn;
+    for (int32_t i = 1; i < len; ++i) {
+      const T v = xb[i];
+      mn = (v < mn || v != v) ? v : mn;
+      mx = (v > mx || v != v) ? v : mx;
+    }
+    bmin[c] = mn;
+    bmax[c] = mx;
+  }
+  __syncthreads();
+  const auto at_k = [line](int32_t k) { return line[k]; };
+  int mine = 0;
+  for (int32_t s = 1 + threadIdx.x; s <= n - 2; s += blockDim.x) {
+    const T cur = line[s], prev = line[s - 1];
+    if (!(prev < cur || prev > cur)) continue;
+    // the run of samples equal to cur from s: samples of s's block, then whole blocks of cur
+    int32_t e;
+    {
+      const int32_t lim = min((s / kBlk) * kBlk + kBlk - 1, n - 1);
+      int32_t k = s + 1;
+      while (k <= lim && line[k] == cur) ++k;
+      if (k <= lim || k >= n) {
+        e = k - 1;
+      } else {
+        e = n - 1;
+        for (int32_t c = k / kBlk; c < nb; ++c) {
+          if (bmin[c] == cur && bmax[c] == cur) continue;
+          k = c * kBlk;
+          while (line[k] == cur) ++k;
+          e = k - 1;
+          break;
+        }
+      }
+    }
+    if (e > n - 2) continue;
+    const T nxt = line[e + 1];
+    const bool is_max = prev < cur && nxt < cur;
+    const bool is_min = prev > cur && nxt > cur;
+    if (!is_max && !is_min) continue;
+    const int32_t pk = (s + e) / 2;
+    const T tp = tau[base + pk];
+    const bool sig = is_max ? side_falls<true, -1>(at_k, n, pk, cur, tp, bmax, bmin) && side_falls<true, 1>(at_k, n, pk, cur, tp, bmax, bmin)
+                            : side_falls<false, -1>(at_k, n, pk, cur, tp, bmin, bmax) && side_falls<false, 1>(at_k, n, pk, cur, tp, bmin, bmax);
+    if (sig) {
+      flags[base + pk] |= static_cast<uint8_t>(1u);
+      ++mine;
+    }
+  }
+  for (int d = 16; d > 0; d >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, d);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&count_s, mine);
+  __syncthreads();
+  if (threadIdx.x == 0 && count_s) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(&el[b].ext[0]), static_cast<unsigned long long>(count_s));
   }
 }
 
@@ -728,38 +806,51 @@ constexpr int32_t kTileWords = 8192;  // int32 parents per tile (32 KiB of share
 
 __device__ __forceinline__ int64_t rows_between(const Geom& g, int a) { return geom_stride(g, a) / g.pitch; }
 
+// A tile is tile_rows consecutive rows of an element, whole (tile_cols = pitch), or for rows longer
+// than a tile (1-D lines beyond kTileWords samples) a run of tile_cols columns of one row.
 __global__ void __launch_bounds__(kThreads) ccl_tiles(Geom g, const uint8_t* __restrict__ mask, uint8_t bits,
-                                                     int32_t* __restrict__ labels, const int32_t* run, int32_t tile_rows) {
+                                                     int32_t* __restrict__ labels, const int32_t* run, int32_t tile_rows,
+                                                     int32_t tile_cols) {
   __shared__ int32_t P[kTileWords];
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
-  const int64_t row0 = static_cast<int64_t>(blockIdx.x) * tile_rows;
+  const int32_t pitch = static_cast<int32_t>(g.pitch), nl = g.n_last;
+  const int32_t col_tiles = (pitch + tile_cols - 1) / tile_cols;
+  const int64_t row0 = static_cast<int64_t>(blockIdx.x / col_tiles) * tile_rows;
+  const int32_t c0 = static_cast<int32_t>(blockIdx.x % col_tiles) * tile_cols;
   if (row0 >= g.rows) return;
   const int32_t rows = static_cast<int32_t>(min(static_cast<int64_t>(tile_rows), g.rows - row0));
-  const int32_t pitch = static_cast<int32_t>(g.pitch), nl = g.n_last;
-  const int32_t words = rows * pitch;
-  const int64_t v0 = row0 * g.pitch;  // the tile's first padded offset in the element
-  const int64_t base = b * g.field + v0;
+  const int32_t cols = min(tile_cols, pitch - c0);
+  const int32_t words = rows * cols;
+  const int64_t v0 = row0 * g.pitch + c0;  // the tile's first padded offset in the element
+  const int64_t eb = b * g.field;
+  // local index k = r cols + c <-> padded offset v0 + r pitch + c
   for (int32_t k = threadIdx.x; k < words; k += blockDim.x) {
-    const int32_t col = k % pitch;
-    P[k] = (col < nl && (mask[base + k] & bits) != 0) ? k : -1;
+    const int32_t r = k / cols, c = k - r * cols;
+    P[k] = (c0 + c < nl && (mask[eb + v0 + static_cast<int64_t>(r) * pitch + c] & bits) != 0) ? k : -1;
   }
   __syncthreads();
   for (int32_t k = threadIdx.x; k < words; k += blockDim.x) {
     if (P[k] < 0) continue;
-    const int32_t r = k / pitch, col = k - r * pitch;
-    if (col + 1 < nl && P[k + 1] >= 0) uf_join<false>(P, k, k + 1);
+    const int32_t r = k / cols, c = k - r * cols;
+    if (c + 1 < cols && c0 + c + 1 < nl && P[k + 1] >= 0) uf_join<false>(P, k, k + 1);
     for (int a = 0; a + 1 < g.dim; ++a) {
       const int64_t rs = rows_between(g, a);
-      if (r + rs >= rows || coord_of(g, v0 + k, a) + 1 >= geom_n(g, a)) continue;
-      const int32_t u = k + static_cast<int32_t>(rs) * pitch;
+      if (r + rs >= rows || coord_of(g, v0 + static_cast<int64_t>(r) * pitch + c, a) + 1 >= geom_n(g, a)) continue;
+      const int32_t u = k + static_cast<int32_t>(rs) * cols;
       if (P[u] >= 0) uf_join<false>(P, k, u);
     }
   }
   __syncthreads();
   for (int32_t k = threadIdx.x; k < words; k += blockDim.x) {
-    const int32_t lab = P[k] < 0 ? -1 : static_cast<int32_t>(v0) + uf_root<false>(P, k);
-    labels[base + k] = lab;
+    const int32_t r = k / cols, c = k - r * cols;
+    int32_t lab = -1;
+    if (P[k] >= 0) {
+      const int32_t root = uf_root<false>(P, k);  // the local root: the smallest local index, so the
+      const int32_t rr = root / cols;             // smallest padded offset of the tile's component
+      lab = static_cast<int32_t>(v0 + static_cast<int64_t>(rr) * pitch + (root - rr * cols));
+    }
+    labels[eb + v0 + static_cast<int64_t>(r) * pitch + c] = lab;
   }
 }
 
@@ -788,7 +879,18 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
     const int32_t LX = (n + ((n - 1) >> 5) + 1) | 1;  // padded line words, odd
     const auto bytes = [&](int p) { return static_cast<size_t>(p) * (LX + 2 * nb) * sizeof(T); };
     while (P > 1 && bytes(P) > cap) P = a == g.dim - 1 ? P - 1 : P / 2;
-    if (bytes(P) > cap) throw std::invalid_argument("edab: a line exceeds the shared memory of the extrema pass");
+    if (bytes(P) > cap) {
+      // a 1-D line beyond the staged capacity: samples from global memory, block extremes staged
+      const size_t ext_bytes = static_cast<size_t>(2) * nb * sizeof(T);
+      if (g.dim != 1 || ext_bytes > cap) throw std::invalid_argument("edab: a line exceeds the shared memory of the extrema pass");
+      if (first_on_device(reinterpret_cast<const void*>(flags_long<T>))) {
+        EDAB_CUDA(cudaFuncSetAttribute(flags_long<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cap)));
+      }
+      flags_long<T><<<dim3(static_cast<unsigned>(g.rows), static_cast<unsigned>(g.batch)), kThreads, ext_bytes, s>>>(
+          g, r, tau, flags, el, run);
+      EDAB_LAUNCH("flags_long");
+      continue;
+    }
     int64_t groups;
     if (a == g.dim - 1) {
       groups = (g.rows + P - 1) / P;
@@ -804,11 +906,14 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
 }
 
 void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32_t* labels, const int32_t* run) {
-  const int32_t tile_rows = static_cast<int32_t>(std::max<int64_t>(1, kTileWords / g.pitch));
-  const int64_t tiles = (g.rows + tile_rows - 1) / tile_rows;
+  const bool wide = g.pitch > kTileWords;
+  const int32_t tile_rows = wide ? 1 : static_cast<int32_t>(kTileWords / g.pitch);
+  const int32_t tile_cols = wide ? kTileWords : static_cast<int32_t>(g.pitch);
+  const int64_t col_tiles = (g.pitch + tile_cols - 1) / tile_cols;
+  const int64_t tiles = (g.rows + tile_rows - 1) / tile_rows * col_tiles;
   if (tiles > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: components: grid too large");
   ccl_tiles<<<dim3(static_cast<unsigned>(tiles), static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(
-      g, mask, bits, labels, run, tile_rows);
+      g, mask, bits, labels, run, tile_rows, tile_cols);
   EDAB_LAUNCH("ccl_tiles");
   // the edges between tiles
   for_voxels(s, g, [=] __device__(int64_t b) { return run == nullptr || run[b] != 0; },
@@ -816,6 +921,10 @@ void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32
                int32_t* L = labels + b * g.field;
                if (L[v] < 0) return;
                const int64_t row = pitch_row(g, v);
+               const int64_t col = v - row * g.pitch;
+               if (wide && (col + 1) % tile_cols == 0 && col + 1 < g.n_last && L[v + 1] >= 0) {
+                 uf_join<true>(L, static_cast<int32_t>(v), static_cast<int32_t>(v + 1));
+               }
                const int64_t tile = row / tile_rows;
                for (int a = 0; a + 1 < g.dim; ++a) {
                  const int64_t rs = geom_stride(g, a) / g.pitch;

@@ -60,6 +60,11 @@ void run_cube(const void* x_dev, int dim, int64_t batch, const int64_t* n, int o
   const unsigned blocks = blocks_for(fe);
   to_padded<T><<<std::min(blocks, 1u << 16), kThreads, 0, s>>>(g, static_cast<const T*>(x_dev), in);
   EDAB_LAUNCH("to_padded");
+  // 1-D lines beyond the staged capacity fold through a global scratch of batch x pitch samples
+  const size_t lb = long_line_scratch_bytes(g, sizeof(T));
+  void* ls = nullptr;
+  if (lb) EDAB_CUDA(cudaMalloc(&ls, lb));
+  set_long_line_scratch(ls, lb);
   CubeArgs<T> a{};
   a.in = in;
   a.out0 = o0;
@@ -77,6 +82,8 @@ void run_cube(const void* x_dev, int dim, int64_t batch, const int64_t* n, int o
     EDAB_LAUNCH("to_dense");
   }
   EDAB_CUDA(cudaStreamSynchronize(s));
+  set_long_line_scratch(nullptr, 0);
+  cudaFree(ls);
   cudaFree(in);
   cudaFree(o0);
   cudaFree(o1);

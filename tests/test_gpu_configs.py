@@ -6,7 +6,8 @@ eda.decompose and eda.decompose_ragged, on seeded samples made by the benchmark'
 - 1-D: the 2048-sample three-tone signal;
 - 2-D: two of the 64 images of 512 x 512 that the benchmark decomposes (the same seed);
 - 3-D: two volumes of 128^3 made by the 256^3 recipe (the trend's width scaled by the side);
-- 1-D ragged: eight signals of the ragged recipe, lengths 256 to 8192;
+- 1-D ragged: eight signals of the ragged recipe, lengths 256 to 8192, and four of 8193 to 65536
+  samples (lines beyond the shared-memory staging);
 - 2-D ragged: four images of uneven sides, 64 to 640, by the ragged 2-D recipe.
 
 For every element:
@@ -104,6 +105,16 @@ def test_config_3d_stand_in(engine):
 
 def test_config_ragged_1d(engine):
     xs = bench.signals_ragged(8, 256, 8192, 2024)
+    rows, infos = engine.decompose_ragged(xs, return_info=True)
+    _check(xs, rows, [(int(i.n_imfs), [int(v) for v in i.windows], [int(v) for v in i.sifts]) for i in infos])
+
+
+def test_config_long_1d_signals(engine):
+    """Signals of the 1-D ragged recipe beyond the 8192 samples that a pass stages in shared memory,
+    up to the recipe's 65536: their lines fold in global memory."""
+    xs = [x for x in bench.signals_ragged(40, 256, 65536, 77) if x.size > 8192][:3]
+    xs.append(bench.signals_ragged(1, 65536, 65536, 5)[0])
+    assert all(x.size > 8192 for x in xs) and xs[-1].size == 65536
     rows, infos = engine.decompose_ragged(xs, return_info=True)
     _check(xs, rows, [(int(i.n_imfs), [int(v) for v in i.windows], [int(v) for v in i.sifts]) for i in infos])
 

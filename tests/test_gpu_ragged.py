@@ -118,7 +118,9 @@ def test_ragged_rejects_a_field_beyond_the_axis_limit(torch):
     import eda
 
     with pytest.raises(ValueError, match="exceeds the limit"):
-        eda.decompose_ragged([signal(300, 1).astype(np.float32), signal(8193, 2).astype(np.float32)])
+        eda.decompose_ragged([signal(300, 1).astype(np.float32), signal(65537, 2).astype(np.float32)])
+    with pytest.raises(ValueError, match="exceeds the limit"):
+        eda.decompose_ragged([np.zeros((8193, 4), np.float32), np.zeros((6, 4), np.float32)])
 
 
 def test_fresh_workspaces_are_zeroed_on_the_workers_streams(torch):

@@ -140,6 +140,26 @@ def test_cube_on_the_longest_lines(dev):
     check(dev, (4096,), "maxmin", [2047, 9], np.float64)
 
 
+# 1-D lines beyond the staged capacity (the long-line pass folds in global memory): every op,
+# one-sample, one-chunk, multi-chunk and clamped windows, up to the 1-D limit of 65536 samples
+LONG_WINS = [1, 3, 31, 33, 1025, 40001, 131071]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", list(OPS))
+@pytest.mark.parametrize("n", [8193, 16384, 65536])
+def test_cube_on_long_1d_lines(dev, n, op, dtype):
+    check(dev, (n,), op, LONG_WINS[:4] if n == 8193 else LONG_WINS, dtype, seed=n)
+
+
+def test_cube_rung_launch_on_long_lines(dev):
+    rng = np.random.default_rng(5)
+    wins = (2 * rng.integers(0, 3000, size=(4, 2)) + 1).astype(np.int32)
+    wins[1, 0] = 0
+    check(dev, (30000,), "maxmin", wins, np.float32, seed=3)
+    check(dev, (30000,), "box", wins, np.float32, seed=4)
+
+
 @pytest.mark.parametrize("k", [1, 2, 5, 32])
 @pytest.mark.parametrize("op", ["maxmin", "box"])
 @pytest.mark.parametrize("shape", [(37, 45), (300,), (11, 9, 14)], ids=["2d", "1d", "3d"])

@@ -156,9 +156,11 @@ def test_select_differences(dev, dtype, shape):
 
 
 def test_select_single_item(dev):
-    x = np.array([[3.5], [-0.0]], np.float32)
-    out, cnt = gpu_select(dev, x)
+    x = np.array([[3.5, 1.0], [-0.0, 2.0]], np.float32)
+    mask = np.array([[1, 0], [1, 0]], np.uint8)
+    out, cnt = gpu_select(dev, x, mask=mask)
     assert list(out) == [3.5, 0.0] and list(cnt) == [1, 1]
+    assert not np.signbit(out[1])  # -0 selects as +0
 
 
 # ---------------------------------------------------------------------------------------------
@@ -217,7 +219,7 @@ def check_flags(dev, r, tau):
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("shape", [(3, 3), (2, 33), (2, 100), (4, 2047), (2, 64, 77), (2, 12, 10, 37)])
+@pytest.mark.parametrize("shape", [(3, 3), (2, 33), (2, 100), (4, 2047), (2, 12000), (2, 64, 77), (2, 12, 10, 37)])
 def test_flags(dev, dtype, kind, shape):
     r = lines(shape, dtype, sum(shape) + len(kind), kind)
     rng = np.random.default_rng(sum(shape))
@@ -227,7 +229,8 @@ def test_flags(dev, dtype, kind, shape):
         check_flags(dev, r, tau)
 
 
-@pytest.mark.parametrize("dtype,n", [(np.float32, 8192), (np.float64, 4096)])
+@pytest.mark.parametrize("dtype,n", [(np.float32, 8192), (np.float64, 4096), (np.float32, 20000), (np.float64, 65536),
+                                     (np.float32, 65536)])
 def test_flags_longest_lines(dev, dtype, n):
     r = lines((2, n), dtype, 11, "smooth")
     tau = np.full(r.shape, 0.4, dtype)
@@ -259,7 +262,8 @@ def gpu_components(dev, mask, bits=1):
     return ld.cpu().numpy()
 
 
-@pytest.mark.parametrize("shape", [(2, 1), (2, 100), (3, 8192), (2, 7, 13), (2, 512, 512), (1, 3000, 70),
+@pytest.mark.parametrize("shape", [(2, 2), (2, 100), (3, 8192), (2, 20000), (1, 65536), (2, 7, 13), (2, 512, 512),
+                                   (1, 3000, 70),
                                    (2, 5, 6, 7), (2, 16, 9, 33), (1, 64, 64, 64)])
 @pytest.mark.parametrize("density", [0.0, 0.3, 0.5, 0.6, 1.0])
 def test_components(dev, shape, density):
