@@ -157,6 +157,29 @@ def _dtype_name(dtype: Any) -> str:
         return str(dtype).removeprefix("torch.")
 
 
+def _stream_handle(stream: Any, default: int | None) -> int:
+    """A raw CUDA stream handle from an int, a torch / CuPy stream object, or the default."""
+    if stream is None:
+        return int(default or 0)
+    for attr in ("cuda_stream", "ptr", "handle"):
+        if hasattr(stream, attr):
+            return int(getattr(stream, attr))
+    return int(stream)
+
+
+def _c_contiguous(shape: Sequence[int], strides: Sequence[int]) -> bool:
+    expect = 1
+    for n, st in zip(reversed(list(shape)), reversed(list(strides))):
+        if n != 1 and st != expect:
+            return False
+        expect *= n
+    return True
+
+
+def _wrap(a: Any) -> Any:
+    return a if isinstance(a, _device.DeviceArray) else _device.DeviceArray(a)
+
+
 def decompose(
     x: Any,
     axes: int | Sequence[int] | None = None,
@@ -188,6 +211,14 @@ def decompose(
     if not isinstance(errors, str) or errors not in ("raise", "status"):
         raise ValueError(f"eda: errors={errors!r} is not one of 'raise', 'status'")
     on_device = _device.is_cuda_array(x)
+    if on_device and not _device.is_torch(x):
+        # any other CUDA array: read through the CUDA array interface or DLPack, without PyTorch
+        cin = _device.intake(x)
+        try:
+            return _decompose_cuda(cin, axes, max_imf, dtype, tie, sifts, check_finite, errors, stream, return_info,
+                                   return_orientation)
+        finally:
+            cin.release()
     if on_device:
         data = _device.as_tensor(x)
         src = _device.dtype_name(data)
@@ -251,6 +282,66 @@ def decompose(
         xt = np.ascontiguousarray(xc.transpose(order)) if order != list(range(ndim)) else xc
         xb = np.ascontiguousarray(xt).reshape((B,) + spatial)
         rows, raw = core.decompose_host(xb, max_imf, tie, sifts, check_finite, return_orientation, 0)
+    return _finish(raw, rows_t if on_device else rows, on_device, batch_shape, batch_axes, axes, spatial, ndim, target,
+                   errors, return_info, return_orientation)
+
+
+def _decompose_cuda(cin, axes, max_imf, dtype, tie, sifts, check_finite, errors, stream, return_info,
+                    return_orientation):
+    """eda.decompose of a CUDA array that is not a torch tensor (DLPack or the CUDA array interface):
+    read in place where it is a C-contiguous array of the compute dtype, else gathered and cast by the
+    engine chunk by chunk (eda_decompose_strided); the results in engine-allocated DeviceArrays. The
+    engine runs on the array's stream (the CUDA array interface's, else ``stream``, else the legacy
+    default stream), so it is ordered after the producer's work."""
+    src = cin.dtype
+    if src not in _device.SUPPORTED_DTYPES:
+        raise TypeError(f"eda: arrays of dtype {src} are not supported (real bool, integer and float arrays only)")
+    target = src if dtype is None else _dtype_name(dtype)
+    if target not in _FLOATS:
+        if dtype is None:
+            raise TypeError(f"eda: expected a float32 or float64 array, got dtype {src} (pass dtype='float32' or "
+                            "dtype='float64' to cast it)")
+        raise TypeError(f"eda: dtype= must be float32 or float64, got {target}")
+    ndim = len(cin.shape)
+    axes = _axes(axes, ndim)
+    if return_orientation and len(axes) < 2:
+        raise ValueError("eda: return_orientation=True needs 2 or 3 spatial axes, got 1 (the method has no "
+                         "orientation in 1-D)")
+    batch_axes = tuple(i for i in range(ndim) if i not in axes)
+    batch_shape = tuple(int(cin.shape[i]) for i in batch_axes)
+    spatial = tuple(int(cin.shape[a]) for a in axes)
+    B = math.prod(batch_shape)
+    order = list(batch_axes) + list(axes)
+    layout = None
+    if not (src == target and _c_contiguous([cin.shape[i] for i in order], [cin.strides[i] for i in order])):
+        layout = (src, batch_shape, tuple(int(cin.strides[i]) for i in batch_axes),
+                  tuple(int(cin.strides[a]) for a in axes))
+    core = _native.core()
+    dev = cin.device
+    if B == 0:
+        rows_t, raw = _device.DeviceArray.empty((0, 1) + spatial, target, dev), core._empty_info(0)
+    else:
+        def alloc(P):
+            out = _device.DeviceArray.empty((B, P) + spatial, target, dev)
+            return out, out.ptr
+
+        def orient_of(K):
+            d = _device.DeviceArray.empty((B, K, len(spatial)) + spatial, target, dev)
+            c = _device.DeviceArray.empty((B, K) + spatial, target, dev)
+            return (d, d.ptr), (c, c.ptr)
+
+        rows_t, raw = core.decompose_device(cin.ptr, dev, target, (B,) + spatial, max_imf, tie, sifts, check_finite,
+                                            0, _stream_handle(stream, cin.stream), alloc,
+                                            orient_of if return_orientation else None, layout)
+    return _finish(raw, rows_t, True, batch_shape, batch_axes, axes, spatial, ndim, target, errors, return_info,
+                   return_orientation)
+
+
+def _finish(raw, rows, on_device, batch_shape, batch_axes, axes, spatial, ndim, target, errors, return_info,
+            return_orientation):
+    """The result of a call: the information, the error policy, the rows in the caller's layout and
+    the orientation."""
+    rows_t = rows
     info = DecompositionInfo(
         n_imfs=np.asarray(raw["n_imfs"], np.int32).reshape(batch_shape),
         error=np.asarray(raw["error"], np.int32).reshape(batch_shape),
@@ -282,7 +373,7 @@ def decompose(
         y_t = rows_t.reshape(batch_shape + (P,) + spatial)
         if perm != list(range(ndim + 1)):
             y_t = y_t.permute(perm)
-        y = _device.DeviceArray(y_t)
+        y = _wrap(y_t)
     else:
         P = rows.shape[1]
         y = rows.reshape(batch_shape + (P,) + spatial)
@@ -301,7 +392,7 @@ def decompose(
             p2 = _restore(ndim, batch_axes, axes, extra)
             if on_device:
                 a = a.reshape(shape)
-                parts.append(_device.DeviceArray(a.permute(p2) if p2 != list(range(len(p2))) else a))
+                parts.append(_wrap(a.permute(p2) if p2 != list(range(len(p2))) else a))
             else:
                 a = np.asarray(a).reshape(shape)
                 parts.append(a.transpose(p2) if p2 != list(range(len(p2))) else a)
@@ -477,14 +568,9 @@ def monogenic(
         torch = _device._torch()
         tdt = getattr(torch, target)
         t = data.permute(order) if order != list(range(ndim)) else data
-        layout = None
-        if t.dtype == tdt and t.is_contiguous():
-            t = t.reshape((B,) + spatial)  # read in place
-        else:
-            # any other element type or layout: the engine gathers and casts each chunk itself
-            # (cpp/src/field/convert.cu:69-170 of the reference), no converted copy of x is made
-            layout = (src, batch_shape, tuple(int(data.stride(i)) for i in batch_axes),
-                      tuple(int(data.stride(a)) for a in axes))
+        # the monogenic call reads C-contiguous arrays of the compute dtype: any other element type
+        # or layout is cast and copied first
+        t = t.to(tdt).contiguous().reshape((B,) + spatial)
         dev = t.device
         flat = torch.empty(planes * B * count, dtype=tdt, device=dev)
         if B:

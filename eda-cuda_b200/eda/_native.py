@@ -79,8 +79,41 @@ class Core:
         L.eda_ragged_free.restype = None
         L.eda_set_transform_precision.argtypes = [ctypes.c_int]
         L.eda_transform_precision.argtypes = []
+        L.eda_buffer_alloc.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+        L.eda_buffer_release.argtypes = [vp]
+        L.eda_buffer_release.restype = None
+        L.eda_buffer_dlpack.argtypes = [vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(vp)]
+        L.eda_copy_to_host.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_int]
+        L.eda_pointer_device.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         self._lib = L
         self.path = str(path)
+
+    # -- device buffers of results (no array library needed) ------------------------------------
+    def buffer_alloc(self, device: int, nbytes: int) -> tuple[int, int]:
+        h, p = ctypes.c_void_p(), ctypes.c_void_p()
+        self._check(self._lib.eda_buffer_alloc(int(device), int(nbytes), ctypes.byref(h), ctypes.byref(p)))
+        return int(h.value), int(p.value or 0)
+
+    def buffer_release(self, handle: int) -> None:
+        self._lib.eda_buffer_release(ctypes.c_void_p(handle))
+
+    def buffer_dlpack(self, handle: int, byte_offset: int, code: int, bits: int, shape, strides) -> int:
+        nd = len(shape)
+        sh = (ctypes.c_int64 * max(nd, 1))(*[int(v) for v in shape])
+        st = (ctypes.c_int64 * max(nd, 1))(*[int(v) for v in strides])
+        out = ctypes.c_void_p()
+        self._check(self._lib.eda_buffer_dlpack(ctypes.c_void_p(handle), int(byte_offset), int(code), int(bits), nd,
+                                                sh, st, ctypes.byref(out)))
+        return int(out.value)
+
+    def copy_to_host(self, dst: int, src: int, nbytes: int, device: int) -> None:
+        self._check(self._lib.eda_copy_to_host(ctypes.c_void_p(dst), ctypes.c_void_p(src), int(nbytes), int(device)))
+
+    def pointer_device(self, ptr: int) -> int:
+        d = ctypes.c_int()
+        self._check(self._lib.eda_pointer_device(ctypes.c_void_p(ptr), ctypes.byref(d)))
+        return int(d.value)
 
     # -- the float32 transforms' product ------------------------------------------------------
     def set_transform_precision(self, mode: int) -> None:

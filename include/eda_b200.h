@@ -175,6 +175,24 @@ EDA_API int eda_device_info(int device, char* buf, size_t len);
  * (the reference's Context::release_unused_memory, cpp/src/runtime/context.cpp:154-160). */
 EDA_API int eda_release_workspace(void);
 
+/* Device buffers for results returned to callers without an array library (the reference's output
+ * pool and DLPack export, cpp/src/runtime/memory.hpp:44-75, src/eda/_device.py:228-334):
+ * eda_buffer_alloc allocates `bytes` on `device` and returns the buffer (one reference, the
+ * caller's) and its pointer; eda_buffer_release drops a reference (the memory is freed with the
+ * last one); eda_buffer_dlpack exports a view of it (byte_offset, DLPack dtype code 0 int / 1 uint /
+ * 2 float / 4 bfloat / 6 bool, bits, ndim <= 8, shape and strides in elements) as a
+ * DLManagedTensor* (DLPack 0.8 ABI) that holds one reference until its deleter runs.
+ * eda_copy_to_host copies device memory of `device` to the host (synchronous). eda_pointer_device
+ * gives the device of device (or managed) memory at p (the reference's pointer_device,
+ * cpp/python/module.cpp), EDA_INVALID_ARGUMENT for other memory. */
+typedef struct eda_buffer eda_buffer;
+EDA_API int eda_buffer_alloc(int device, size_t bytes, eda_buffer** out, void** ptr);
+EDA_API void eda_buffer_release(eda_buffer* b);
+EDA_API int eda_buffer_dlpack(eda_buffer* b, size_t byte_offset, int dtype_code, int bits, int ndim,
+                              const int64_t* shape, const int64_t* strides, void** managed);
+EDA_API int eda_copy_to_host(void* dst, const void* src, size_t bytes, int device);
+EDA_API int eda_pointer_device(const void* p, int* device);
+
 /* The product of the float32 orientation transforms, process-wide (no counterpart in the reference,
  * whose transforms are cuFFT's float32 FFTs, cpp/src/method/orientation.cu:674-767): 0 = 3xTF32
  * split products on the tensor cores (the default), 1 = BF16x3 split products on the tensor cores,
