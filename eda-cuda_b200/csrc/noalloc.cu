@@ -7,8 +7,7 @@
 // its scratch memory in the file-scope device array below.
 //
 // The call is synchronous: the engine reads per-element state back to the host between the steps
-// of a mode and at the end of the call, so it blocks the host on the caller's stream several times
-// and cannot be recorded into a CUDA graph by stream capture.
+// of a mode and at the end of the call, so it blocks the host on the caller's stream several times.
 //
 // The array (kScratchBytes per device) is part of the library's image: every GPU that loads the
 // library holds it until the process exits. Every call shares it, and it keeps the last call's

@@ -216,8 +216,7 @@ EDA_API int eda_transform_precision(void);
  * length up to about 32768 float32 or 16384 float64 samples; larger calls are rejected with
  * EDA_INVALID_ARGUMENT, as are buffers that are not device memory of the current device. The first
  * call on a device looks the array's address up. The call is synchronous: it blocks the host on the
- * stream several times (per-element state is read back between the steps of a mode), so it cannot
- * be recorded into a CUDA graph by stream capture. Calls share the array: calls that overlap on the
+ * stream several times (per-element state is read back between the steps of a mode). Calls share the array: calls that overlap on the
  * GPU race, so serialize them. It calls no cudaMalloc, cudaFree or allocating library routine. */
 EDA_API int eda_decompose_noalloc(const void* x_dev, int dtype, int64_t batch, int64_t length,
                                   const eda_params* params, void* rows_dev, int32_t rows_capacity, int32_t* rows,
