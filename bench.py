@@ -384,6 +384,9 @@ def other_workload(name: str, seed: int):
         return ("3-D 4 x 256^3 float32 (spherical waves, chirped plane wave, trend, noise), sifts 3",
                 volumes_3d(4, 256, seed), (1, 2, 3), 4)
     if name == "ragged1d":
+        return ("1-D ragged 1024 signals, lengths exp(U[ln 256, ln 65536]) float32 (chirp, FM tone, slope, noise), "
+                "sifts 3", signals_ragged(1024, 256, 65536, seed), None, 1024)
+    if name == "ragged1d-short":
         return ("1-D ragged 1024 signals, lengths exp(U[ln 256, ln 8192]) float32 (chirp, FM tone, slope, noise), "
                 "sifts 3", signals_ragged(1024, 256, 8192, seed), None, 1024)
     if name == "ragged2d":
@@ -419,9 +422,24 @@ def fp64_error(fields: list[np.ndarray], results: list[np.ndarray], threads: int
             "n_checked": len(ok), "decisions_differ": len(out) - len(ok), "oracle": "float64 restatement of the sift"}
 
 
+def check_fields(name: str, data) -> tuple[list[np.ndarray], tuple | None, str]:
+    """The seeded subset whose rows are checked against the float64 oracle, with its axes (None:
+    ragged) and a description: the whole 1-D workload; one 128^3 volume of the 3-D recipe (a 256^3
+    volume takes the oracle minutes); four fields of the ragged workloads (the shortest)."""
+    if name == "1d":
+        return [data[0]], (1,), "the signal"
+    if name == "3d":
+        return [volumes_3d(1, 128, 7)[0]], (1, 2, 3), "one 128^3 volume of the same recipe (seed 7)"
+    order = sorted(range(len(data)), key=lambda i: data[i].size)[:4]
+    return [data[i] for i in order], None, "the four smallest fields of the batch"
+
+
 def run_other(args) -> None:
     """One JSON line for a configuration other than the 2-D benchmark (1 GPU): decompositions/s with
-    device-resident inputs (CUDA events around each call) and through host inputs (e2e)."""
+    device-resident inputs (CUDA events around each call) and through host inputs (e2e). For 2-D and
+    3-D workloads every product of the float32 orientation transforms is timed too ("arms": 3xTF32
+    and BF16x3 split products on the tensor cores, plain float32), each with its float64 error; the
+    line's value is the default arm's (3xTF32)."""
     import torch
 
     import eda
@@ -463,6 +481,43 @@ def run_other(args) -> None:
         wall.append(1000 * (time.perf_counter() - t0))
         d2h = sum(np.asarray(r).nbytes for r in out) if ragged else out.nbytes
     total = sum(ms)
+    # the float64 error of a seeded subset, outside the timed regions
+    fields, faxes, fdesc = check_fields(args.workload, data)
+
+    def subset_err():
+        if faxes is None:
+            ys = eda.decompose_ragged(fields)
+        else:
+            y = eda.decompose(np.stack(fields), axes=faxes)
+            ys = [y[b] for b in range(len(fields))]
+        err = fp64_error(fields, ys, max(1, min(host_cores(), len(fields))))
+        err["sample"] = fdesc
+        return err
+
+    arms = None
+    spatial_dims = len(axes) if axes is not None else data[0].ndim
+    if spatial_dims >= 2 and not args.no_cpu:
+        arms = {}
+        for arm in eda.TRANSFORM_PRECISIONS:
+            eda.set_transform_precision(arm)
+            for _ in range(max(1, args.warmup)):
+                call_dev()
+            torch.cuda.synchronize(dev)
+            am = []
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                call_dev()
+                e1.record()
+                e1.synchronize()
+                am.append(e0.elapsed_time(e1))
+            arms[arm] = {"value": elements * args.steps / (sum(am) / 1000.0), "ms_per_step": sum(am) / args.steps,
+                         "fp64_err": subset_err()}
+        eda.set_transform_precision("tf32x3")
+        arms["ratio_tf32x3_vs_fp32"] = arms["tf32x3"]["value"] / arms["fp32"]["value"]
+        arms["ratio_bf16x3_vs_fp32"] = arms["bf16x3"]["value"] / arms["fp32"]["value"]
+    err = arms["tf32x3"]["fp64_err"] if arms else (subset_err() if not args.no_cpu else None)
     line = {
         "metric": f"decompositions/s ({args.workload})", "value": elements * args.steps / (total / 1000.0),
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
@@ -471,6 +526,8 @@ def run_other(args) -> None:
         "e2e": {"value": elements * args.steps / (sum(wall) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
+        "fp64_err": err,
+        "arms": arms,
     }
     print(json.dumps(line), flush=True)
 
@@ -510,7 +567,7 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling runs)")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="images per GPU of the 2-D benchmark (64; smaller only for profiling captures)")
-    ap.add_argument("--workload", default="2d", choices=("2d", "1d", "3d", "ragged1d", "ragged2d"),
+    ap.add_argument("--workload", default="2d", choices=("2d", "1d", "3d", "ragged1d", "ragged1d-short", "ragged2d"),
                     help="2d: the benchmark (default); the others measure the remaining configurations on 1 GPU")
     ap.add_argument("--traffic-from", metavar="CSV",
                     help="write the cube passes' DRAM bytes per launch from an ncu --csv log of "
