@@ -40,6 +40,11 @@ namespace {
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxGroupsPerCta = 1;  // line groups one CTA runs at most (measured: 1 is fastest)
+// A window folds whole segments per worker when its segments number at least workers / kSeqShare.
+#ifndef EDAB_SEQ_SHARE
+#define EDAB_SEQ_SHARE 4
+#endif
+constexpr int kSeqShare = EDAB_SEQ_SHARE;
 
 __host__ __device__ constexpr int32_t tot_slots(int32_t n) { return n / 8 + 24; }
 // Line stride of the row layout in elements: the padded row rounded up, plus 16 bytes (4 words
@@ -167,8 +172,10 @@ __device__ __forceinline__ T chunk_total(const T* __restrict__ vp) {
   return loc;
 }
 // H of the chunk into its output slots (one slot back per sample): carry op local.
+// Every chunk fold returns its last fold value: the chunk's local total for sums, the fold from the
+// carry for max / min (a segment folded chunk after chunk chains its carries from these).
 template <class T, int OP, int PP>
-__device__ __forceinline__ void chunk_h(const T* __restrict__ vp, T* __restrict__ rp, T cv) {
+__device__ __forceinline__ T chunk_h(const T* __restrict__ vp, T* __restrict__ rp, T cv) {
   if constexpr (OP == kOpSum) {
     T loc = vp[0];
     rp[0] = add_rn(cv, loc);
@@ -177,6 +184,7 @@ __device__ __forceinline__ void chunk_h(const T* __restrict__ vp, T* __restrict_
       loc = add_rn(loc, vp[-s * PP]);
       rp[-s * PP] = add_rn(cv, loc);
     }
+    return loc;
   } else {
     T loc = cv;
 #pragma unroll
@@ -184,12 +192,13 @@ __device__ __forceinline__ void chunk_h(const T* __restrict__ vp, T* __restrict_
       loc = fop<OP>(loc, vp[-s * PP]);
       rp[-s * PP] = loc;
     }
+    return loc;
   }
 }
 // G of the chunk combined with the H already in its output slots; the segment's last sample of an
 // aligned box window (aligned_end) takes (H + G) * 0.5.
 template <class T, int OP, int PP>
-__device__ __forceinline__ void chunk_g(const T* __restrict__ vp, T* __restrict__ rp, T cv, bool aligned_end) {
+__device__ __forceinline__ T chunk_g(const T* __restrict__ vp, T* __restrict__ rp, T cv, bool aligned_end) {
   if constexpr (OP == kOpSum) {
     T loc = vp[0];
 #pragma unroll
@@ -198,6 +207,7 @@ __device__ __forceinline__ void chunk_g(const T* __restrict__ vp, T* __restrict_
       const T y = add_rn(rp[s * PP], add_rn(cv, loc));
       rp[s * PP] = (s == 31 && aligned_end) ? mul_rn(y, T(0.5)) : y;
     }
+    return loc;
   } else {
     T loc = cv;
 #pragma unroll
@@ -205,6 +215,7 @@ __device__ __forceinline__ void chunk_g(const T* __restrict__ vp, T* __restrict_
       loc = fop<OP>(loc, vp[s * PP]);
       rp[s * PP] = fop<OP>(rp[s * PP], loc);
     }
+    return loc;
   }
 }
 
@@ -236,8 +247,8 @@ __device__ __forceinline__ T partial_total(const T* __restrict__ v, int32_t len)
 }
 // H: the output of sample i is stored (slots step back with the samples: STEP = -PP for both)
 template <class T, int OP, int PP>
-__device__ __forceinline__ void partial_h(const T* __restrict__ v, T* __restrict__ r, int32_t len, int32_t skip,
-                                          T cv) {
+__device__ __forceinline__ T partial_h(const T* __restrict__ v, T* __restrict__ r, int32_t len, int32_t skip,
+                                       T cv) {
   T loc = fold_init<T, OP>(cv, v[0]);
   if (skip == 0) r[0] = fold_out<T, OP>(cv, loc);
   int32_t i = 1;
@@ -254,6 +265,7 @@ __device__ __forceinline__ void partial_h(const T* __restrict__ v, T* __restrict
     loc = fop<OP>(loc, v[-i * PP]);
     r[-i * PP] = fold_out<T, OP>(cv, loc);
   }
+  return loc;
 }
 // G combined with the H in the slots (STEP = +PP); the chunk's last sample, when it ends an aligned
 // box window (aligned_end), takes (H + G) * 0.5.
@@ -267,13 +279,13 @@ __device__ __forceinline__ void combine_g(T* __restrict__ slot, T cv, T loc, boo
   }
 }
 template <class T, int OP, int PP>
-__device__ __forceinline__ void partial_g(const T* __restrict__ v, T* __restrict__ r, int32_t len, int32_t skip,
-                                          T cv, bool aligned_end) {
+__device__ __forceinline__ T partial_g(const T* __restrict__ v, T* __restrict__ r, int32_t len, int32_t skip,
+                                       T cv, bool aligned_end) {
   const int32_t last = len - 1;
   T loc = fold_init<T, OP>(cv, v[0]);
   if (last == 0) {
     if (skip == 0) combine_g<T, OP>(r, cv, loc, aligned_end);
-    return;
+    return loc;
   }
   if (skip == 0) combine_g<T, OP>(r, cv, loc, false);
   int32_t i = 1;
@@ -292,6 +304,71 @@ __device__ __forceinline__ void partial_g(const T* __restrict__ v, T* __restrict
   }
   loc = fop<OP>(loc, v[last * PP]);
   if (last >= skip) combine_g<T, OP>(r + last * PP, cv, loc, aligned_end);
+  return loc;
+}
+
+// The carry into the next chunk of a segment from this chunk's fold value (the canonical chunk
+// carries: the first chunk's total, then carry op total; max / min values already hold the carry).
+template <class T, int OP>
+__device__ __forceinline__ T next_carry(T carry, T loc, bool first) {
+  if constexpr (OP == kOpSum) return first ? loc : add_rn(carry, loc);
+  else return fop<OP>(carry, loc);
+}
+
+// A whole segment [s, e_last] folded by one worker, chunk after chunk with the carries chained (no
+// chunk totals pass, no carry pass): H of the reversed line into the output slots n - 1 + r - e,
+// then (after the CTA's barrier) G combined with them.
+template <class T, int OP, int PP>
+__device__ __forceinline__ void seg_h(const T* __restrict__ Vp, T* __restrict__ Rp, int32_t n, const Win& q,
+                                      int32_t s, int32_t e_last) {
+  T carry = fold_identity<T, OP>();
+  for (int32_t c = 0, c0 = s; c0 <= e_last; ++c, c0 += 32) {
+    const int32_t c1 = min(c0 + 31, e_last);
+    T loc;
+    if (c0 >= 0 && c1 <= n - 1) {
+      const T* vp = Vp + (n - 1 - c0) * PP;
+      T* rp = Rp + (n - 1 + q.r - c0) * PP;
+      if (c1 == c0 + 31 && c0 >= q.r) loc = chunk_h<T, OP, PP>(vp, rp, carry);
+      else loc = partial_h<T, OP, PP>(vp, rp, c1 - c0 + 1, max(0, q.r - c0), carry);
+    } else {
+      const T cv = carry;
+      loc = fold_chunk<T, OP>(Vp, PP, n, c0, c1, 1, [&](int32_t e, T l) {
+        if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = fop<OP>(cv, l);
+      });
+    }
+    carry = next_carry<T, OP>(carry, loc, c == 0);
+  }
+}
+template <class T, int OP, int PP>
+__device__ __forceinline__ void seg_g(const T* __restrict__ Vp, T* __restrict__ Rp, int32_t n, const Win& q,
+                                      int32_t s, int32_t e_last) {
+  const int32_t e_al = s + q.wa - 1;
+  T carry = fold_identity<T, OP>();
+  for (int32_t c = 0, c0 = s; c0 <= e_last; ++c, c0 += 32) {
+    const int32_t c1 = min(c0 + 31, e_last);
+    T loc;
+    if (c0 >= 0 && c1 <= n - 1) {
+      const T* vp = Vp + c0 * PP;
+      T* rp = Rp + (c0 - q.r) * PP;
+      if (c1 == c0 + 31 && c0 >= q.r) loc = chunk_g<T, OP, PP>(vp, rp, carry, c1 == e_al);
+      else loc = partial_g<T, OP, PP>(vp, rp, c1 - c0 + 1, max(0, q.r - c0), carry, c1 == e_al);
+    } else {
+      const T cv = carry;
+      loc = fold_chunk<T, OP>(Vp, PP, n, c0, c1, 0, [&](int32_t e, T l) {
+        if (e < q.r) return;
+        const T g = fop<OP>(cv, l);
+        T* slot = Rp + (e - q.r) * PP;
+        const T h = *slot;
+        if constexpr (OP == kOpSum) {
+          const T sum = add_rn(h, g);
+          *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+        } else {
+          *slot = fop<OP>(h, g);
+        }
+      });
+    }
+    carry = next_carry<T, OP>(carry, loc, c == 0);
+  }
 }
 
 // The fold tasks (segment k, chunk c) of one worker, chunk-major (u = c nseg + k, u = first,
@@ -346,9 +423,26 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     __syncthreads();
     return;
   }
-  // segments of one chunk (wa <= 32) run in runs of `per` consecutive segments, one run per task
-  // (about one task per worker): a task's set-up is paid once per run, not once per segment
-  const int32_t per = q.cps == 1 ? (q.nseg + workers - 1) / workers : 1;
+  // Windows of many segments per line: every worker folds whole segments (a run of `per` of them,
+  // about one run per worker), chunk after chunk with chained carries, in two barrier-separated
+  // phases. Windows of few, long segments (kSeqShare * nseg < workers) split their segments into
+  // chunks over the workers instead: chunk totals, carries, then the H and G folds (four phases,
+  // twice the folds, but every worker busy).
+  if (q.cps == 1 || q.nseg * kSeqShare >= workers) {
+    const int32_t per = (q.nseg + workers - 1) / workers;
+    const int32_t k_end = min((worker + 1) * per, q.nseg);
+    for (int32_t k = worker * per; k < k_end; ++k) {
+      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+      seg_h<T, OP, PP>(Vp, Rp, n, q, s, min(s + q.wa - 1, e_max));
+    }
+    __syncthreads();
+    for (int32_t k = worker * per; k < k_end; ++k) {
+      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+      seg_g<T, OP, PP>(Vp, Rp, n, q, s, min(s + q.wa - 1, e_max));
+    }
+    __syncthreads();
+    return;
+  }
   if (q.cps > 1) {
     // phase 1: chunk totals; half of the workers take the line, half the reversed line
     constexpr int half = workers / 2;
@@ -392,20 +486,6 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     __syncthreads();
   }
   // phase 3: H (the reversed line's G) into R at the output slots n - 1 + r - e (e >= r)
-  if (per > 1) {
-    const int32_t k_end = min((worker + 1) * per, q.nseg);
-    for (int32_t k = worker * per; k < k_end; ++k) {
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
-      const int32_t c1 = min(s + q.wa - 1, e_max);
-      if (s >= 0 && c1 <= n - 1) {
-        partial_h<T, OP, PP>(Vp + (n - 1 - s) * PP, Rp + (n - 1 + q.r - s) * PP, c1 - s + 1, max(0, q.r - s), idn);
-      } else {
-        fold_chunk<T, OP>(Vp, PP, n, s, c1, 1, [&](int32_t e, T loc) {
-          if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = fop<OP>(idn, loc);
-        });
-      }
-    }
-  } else
   for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
     const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
@@ -426,30 +506,6 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   }
   __syncthreads();
   // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r)), slot x = e - r
-  if (per > 1) {
-    const int32_t k_end = min((worker + 1) * per, q.nseg);
-    for (int32_t k = worker * per; k < k_end; ++k) {
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
-      const int32_t e_al = s + q.wa - 1;
-      const int32_t c1 = min(e_al, e_max);
-      if (s >= 0 && c1 <= n - 1) {
-        partial_g<T, OP, PP>(Vp + s * PP, Rp + (s - q.r) * PP, c1 - s + 1, max(0, q.r - s), idn, c1 == e_al);
-      } else {
-        fold_chunk<T, OP>(Vp, PP, n, s, c1, 0, [&](int32_t e, T loc) {
-          if (e < q.r) return;
-          const T g = fop<OP>(idn, loc);
-          T* slot = Rp + (e - q.r) * PP;
-          const T h = *slot;
-          if constexpr (OP == kOpSum) {
-            const T sum = add_rn(h, g);
-            *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
-          } else {
-            *slot = fop<OP>(h, g);
-          }
-        });
-      }
-    }
-  } else
   for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
     const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
     const int32_t e_al = s + q.wa - 1;

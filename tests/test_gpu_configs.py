@@ -113,7 +113,7 @@ def test_config_long_1d_signals(engine):
     """Signals of the 1-D ragged recipe beyond the 8192 samples that a pass stages in shared memory,
     up to the recipe's 65536: their lines fold in global memory."""
     xs = [x for x in bench.signals_ragged(40, 256, 65536, 77) if x.size > 8192][:3]
-    xs.append(bench.signals_ragged(1, 65536, 65536, 5)[0])
+    xs.append(bench.signals_ragged(1, 65536, 65537, 5)[0])  # exp(U[ln 65536, ln 65537]) truncates to 65536
     assert all(x.size > 8192 for x in xs) and xs[-1].size == 65536
     rows, infos = engine.decompose_ragged(xs, return_info=True)
     _check(xs, rows, [(int(i.n_imfs), [int(v) for v in i.windows], [int(v) for v in i.sifts]) for i in infos])
