@@ -39,7 +39,10 @@ namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxGroupsPerCta = 1;  // line groups one CTA runs at most (measured: 1 is fastest)
+#ifndef EDAB_GROUPS_PER_CTA
+#define EDAB_GROUPS_PER_CTA 1
+#endif
+constexpr int kMaxGroupsPerCta = EDAB_GROUPS_PER_CTA;  // line groups one CTA runs at most (measured: 1 is fastest)
 // A window folds whole segments per worker when its segments number at least workers / kSeqShare.
 #ifndef EDAB_SEQ_SHARE
 #define EDAB_SEQ_SHARE 4
@@ -433,12 +436,40 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     const int32_t k_end = min((worker + 1) * per, q.nseg);
     for (int32_t k = worker * per; k < k_end; ++k) {
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
-      seg_h<T, OP, PP>(Vp, Rp, n, q, s, min(s + q.wa - 1, e_max));
+      const int32_t c1 = min(s + q.wa - 1, e_max);
+      if (q.cps > 1) {
+        seg_h<T, OP, PP>(Vp, Rp, n, q, s, c1);
+      } else if (s >= 0 && c1 <= n - 1) {  // a one-chunk segment inside the line
+        partial_h<T, OP, PP>(Vp + (n - 1 - s) * PP, Rp + (n - 1 + q.r - s) * PP, c1 - s + 1, max(0, q.r - s), idn);
+      } else {
+        fold_chunk<T, OP>(Vp, PP, n, s, c1, 1, [&](int32_t e, T loc) {
+          if (e >= q.r) Rp[(n - 1 + q.r - e) * PP] = fop<OP>(idn, loc);
+        });
+      }
     }
     __syncthreads();
     for (int32_t k = worker * per; k < k_end; ++k) {
       const int32_t s = q.o + (q.k_lo + k) * q.wa;
-      seg_g<T, OP, PP>(Vp, Rp, n, q, s, min(s + q.wa - 1, e_max));
+      const int32_t e_al = s + q.wa - 1;
+      const int32_t c1 = min(e_al, e_max);
+      if (q.cps > 1) {
+        seg_g<T, OP, PP>(Vp, Rp, n, q, s, c1);
+      } else if (s >= 0 && c1 <= n - 1) {
+        partial_g<T, OP, PP>(Vp + s * PP, Rp + (s - q.r) * PP, c1 - s + 1, max(0, q.r - s), idn, c1 == e_al);
+      } else {
+        fold_chunk<T, OP>(Vp, PP, n, s, c1, 0, [&](int32_t e, T loc) {
+          if (e < q.r) return;
+          const T gv = fop<OP>(idn, loc);
+          T* slot = Rp + (e - q.r) * PP;
+          const T h = *slot;
+          if constexpr (OP == kOpSum) {
+            const T sum = add_rn(h, gv);
+            *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+          } else {
+            *slot = fop<OP>(h, gv);
+          }
+        });
+      }
     }
     __syncthreads();
     return;
