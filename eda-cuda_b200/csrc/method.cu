@@ -319,6 +319,15 @@ __global__ void __launch_bounds__(kThreads) element_rungs(Geom g, uint8_t* lo, T
 // lie in rung0 (rung1: the min cubes) at j * B * field.
 // Segment point q of a voxel (q = 0..3: x + (1/2) o, x - (1/2) o, x + o, x - o): per axis the
 // offsets (in the element, reflected) of the two interpolation neighbours and their weights.
+// The gathers' launch shape: CTAs of 256 threads per SM (the register bound) and how many of a
+// voxel's four segment points are read together (more loads in flight, more registers).
+#ifndef EDAB_GATHER_CTAS
+#define EDAB_GATHER_CTAS 6
+#endif
+#ifndef EDAB_GATHER_UNROLL
+#define EDAB_GATHER_UNROLL 1
+#endif
+constexpr int kGatherUnroll = EDAB_GATHER_UNROLL;
 template <class T, int D>
 struct SegPoint {
   int32_t off0[D], off1[D];
@@ -386,7 +395,7 @@ __device__ __forceinline__ T gather_op(T acc, T v, bool second) {
 }
 
 template <class T, int D, int OP>
-__global__ void __launch_bounds__(kThreads, 6) gather_kernel(Geom g, const Elem* __restrict__ el,
+__global__ void __launch_bounds__(kThreads, EDAB_GATHER_CTAS) gather_kernel(Geom g, const Elem* __restrict__ el,
                                                          const int32_t* __restrict__ run, const uint8_t* __restrict__ lo,
                                                          const T* __restrict__ t, const T* __restrict__ o0,
                                                          const T* __restrict__ o1, const T* __restrict__ o2,
@@ -429,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 6) gather_kernel(Geom g, const Elem*
           if constexpr (D >= 3) ov[2] = static_cast<double>(__ldg(o2 + at));
 #pragma unroll
           for (int a = 0; a < D; ++a) xd[a] = static_cast<double>(x[a]);
-#pragma unroll 1
+#pragma unroll kGatherUnroll
           for (int q = 0; q < 4; ++q) {
             const SegPoint<T, D> P = seg_point<T, D>(g, xd, ov, q);
             if (pts0) {
