@@ -85,3 +85,72 @@ def decompose_sharded(x: np.ndarray, group: Any = None, gather: bool = True,
     for k in ("windows", "sifts", "spacing", "energy"):
         merged[k] = merged[k][:, :Kw]
     return y, merged
+
+
+def mode_bound(n_max: int) -> int:
+    """The largest number of modes of a field whose longest axis has n_max samples (the window rule
+    of cpp/src/method/driver.cpp:128-140: windows from 3, at least the previous + 2, at least twice
+    the previous from the third mode on, while within n_max)."""
+    w_prev, count = 1, 0
+    k = 0
+    while True:
+        w = max(3, w_prev + 2)
+        if k >= 2:
+            w = max(w, 2 * (int(2.0 * w_prev) // 2) + 1)
+        if w > n_max:
+            return count
+        count += 1
+        w_prev = w
+        k += 1
+
+
+def ragged_assignment(shapes: list[tuple[int, ...]], world: int) -> list[int]:
+    """The rank of every field of a ragged batch: the fields' costs (samples x mode bound, the
+    sift's work) spread over the ranks by longest-processing-time first (each field, heaviest
+    first, to the least loaded rank; ties to the lowest rank), so every rank gets about the same
+    work however uneven the fields are."""
+    if world < 1:
+        raise ValueError("eda: world must be >= 1")
+    cost = [int(np.prod(s)) * max(1, mode_bound(max(s))) for s in shapes]
+    order = sorted(range(len(shapes)), key=lambda i: (-cost[i], i))
+    load = [0] * world
+    rank = [0] * len(shapes)
+    for i in order:
+        r = min(range(world), key=lambda j: (load[j], j))
+        rank[i] = r
+        load[r] += cost[i]
+    return rank
+
+
+def decompose_ragged_sharded(xs: list[np.ndarray], group: Any = None, gather: bool = True,
+                             decompose: Callable[..., tuple[list, list]] | None = None,
+                             **kwargs: Any) -> tuple[list, list]:
+    """Decompose this rank's share of the ragged batch xs (host fields of different shapes, the
+    share from ragged_assignment) and, with gather, return every field's rows and information on
+    every rank, in input order (else this rank's, None elsewhere). The compute call is
+    ``decompose(fields, **kwargs) -> (rows list, infos list)`` (default: eda.decompose_ragged with
+    return_info). The results are collected with all_gather_object (pickled host arrays)."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    owner = ragged_assignment([tuple(np.shape(x)) for x in xs], world)
+    mine = [i for i in range(len(xs)) if owner[i] == rank]
+    if decompose is None:
+        from ._api import decompose_ragged
+
+        def decompose(fields, **kw):
+            return decompose_ragged(fields, return_info=True, **kw)
+    rows_m, infos_m = decompose([xs[i] for i in mine], **kwargs) if mine else ([], [])
+    rows: list = [None] * len(xs)
+    infos: list = [None] * len(xs)
+    for j, i in enumerate(mine):
+        rows[i], infos[i] = rows_m[j], infos_m[j]
+    if not gather or world == 1:
+        return rows, infos
+    parts: list = [None] * world
+    dist.all_gather_object(parts, [(i, np.asarray(rows[i]), infos[i]) for i in mine], group=group)
+    for part in parts:
+        for i, r, inf in part:
+            rows[i], infos[i] = r, inf
+    return rows, infos

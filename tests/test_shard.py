@@ -83,3 +83,84 @@ def test_two_gloo_ranks_gather_the_single_process_result():
         for k in ("n_imfs", "error", "windows", "sifts", "spacing", "energy"):
             assert np.array_equal(info[k], want_info[k]), k
     assert want_info["error"][3] == 1
+
+
+def test_mode_bound_matches_the_oracle():
+    import oracle
+    from eda._shard import mode_bound
+
+    for n in (2, 3, 4, 9, 100, 512, 2048, 8192, 65536):
+        assert mode_bound(n) + 2 == oracle.rows_cap((n,))
+
+
+def test_ragged_assignment_balances_the_work():
+    from eda._shard import mode_bound, ragged_assignment
+
+    rng = np.random.default_rng(3)
+    shapes = [(int(np.exp(rng.uniform(np.log(256), np.log(65536)))),) for _ in range(300)]
+    for world in (1, 2, 3, 8):
+        owner = ragged_assignment(shapes, world)
+        load = [0] * world
+        for s, r in zip(shapes, owner):
+            load[r] += s[0] * mode_bound(s[0])
+        heaviest = max(s[0] * mode_bound(s[0]) for s in shapes)
+        assert max(load) - min(load) <= heaviest  # the longest-processing-time bound
+
+
+def _ragged_fields() -> list[np.ndarray]:
+    rng = np.random.default_rng(9)
+    out = []
+    for n in (300, 1200, 77, 640, 2000, 150):
+        t = np.arange(n)
+        out.append((np.sin(2 * np.pi * t / 11) + 0.5 * np.sin(2 * np.pi * t / 57) + 0.1 * rng.standard_normal(n))
+                   .astype(np.float32))
+    return out
+
+
+def _oracle_ragged(fields, **kw):
+    import oracle
+
+    rows, infos = [], []
+    for x in fields:
+        r, info = oracle.decompose(x[None])
+        rows.append(r[0])
+        infos.append({k: v[0] for k, v in info.items()})
+    return rows, infos
+
+
+def _ragged_worker(rank: int, world: int, port: int, out: dict) -> None:
+    sys.path.insert(0, str(ROOT / "eda-cuda_b200"))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import torch.distributed as dist
+
+    from eda._shard import decompose_ragged_sharded
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        out[rank] = decompose_ragged_sharded(_ragged_fields(), decompose=_oracle_ragged)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_share_a_ragged_batch():
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as manager:
+        out = manager.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_ragged_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+        assert all(p.exitcode == 0 for p in procs)
+        res = dict(out)
+    want_rows, want_infos = _oracle_ragged(_ragged_fields())
+    for rank in (0, 1):
+        rows, infos = res[rank]
+        for got, want in zip(rows, want_rows):
+            assert np.array_equal(got, want, equal_nan=True)
+        for got, want in zip(infos, want_infos):
+            for k in ("n_imfs", "error", "windows", "sifts"):
+                assert np.array_equal(np.asarray(got[k]), np.asarray(want[k])), k
