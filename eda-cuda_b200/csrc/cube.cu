@@ -39,15 +39,10 @@ namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
 constexpr int kWarps = kThreads / 32;
-#ifndef EDAB_GROUPS_PER_CTA
-#define EDAB_GROUPS_PER_CTA 1
-#endif
-constexpr int kMaxGroupsPerCta = EDAB_GROUPS_PER_CTA;  // line groups one CTA runs at most (measured: 1 is fastest)
-// A window folds whole segments per worker when its segments number at least workers / kSeqShare.
-#ifndef EDAB_SEQ_SHARE
-#define EDAB_SEQ_SHARE 4
-#endif
-constexpr int kSeqShare = EDAB_SEQ_SHARE;
+constexpr int kMaxGroupsPerCta = 4;  // line groups one CTA may run (the default launch shape runs one)
+// A window folds whole segments per worker when its segments number at least workers / seq_share
+// (the default, or the tuned value of the geometry).
+constexpr int kSeqShare = 4;
 
 __host__ __device__ constexpr int32_t tot_slots(int32_t n) { return n / 8 + 24; }
 // Line stride of the row layout in elements: the padded row rounded up, plus 16 bytes (4 words
@@ -406,7 +401,7 @@ struct Tasks {
 // chunk totals / carries [2][TS][P] (slot k cps + c). Workers: P lanes each (lane % P = the line).
 template <class T, int OP, int P, int PP>
 __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int32_t n,
-                                          int32_t TS, const Win& q, int32_t LS) {
+                                          int32_t TS, const Win& q, int32_t LS, int32_t seq_share) {
   constexpr int slots = 32 / P;
   constexpr int workers = kWarps * slots;
   const int lane = threadIdx.x & 31;
@@ -428,10 +423,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   }
   // Windows of many segments per line: every worker folds whole segments (a run of `per` of them,
   // about one run per worker), chunk after chunk with chained carries, in two barrier-separated
-  // phases. Windows of few, long segments (kSeqShare * nseg < workers) split their segments into
+  // phases. Windows of few, long segments (seq_share * nseg < workers) split their segments into
   // chunks over the workers instead: chunk totals, carries, then the H and G folds (four phases,
   // twice the folds, but every worker busy).
-  if (q.cps == 1 || q.nseg * kSeqShare >= workers) {
+  if (q.cps == 1 || q.nseg * seq_share >= workers) {
     const int32_t per = (q.nseg + workers - 1) / workers;
     const int32_t k_end = min((worker + 1) * per, q.nseg);
     for (int32_t k = worker * per; k < k_end; ++k) {
@@ -589,6 +584,7 @@ struct PassArgs {
   int32_t vec;            // every pointer and stride allows 16-byte copies
   int64_t groups;         // line groups per element
   int32_t gpc;            // line groups per CTA (blockIdx.x runs groups [x gpc, x gpc + gpc))
+  int32_t seq_share;      // windows of at least workers / seq_share segments fold whole segments
   unsigned long long* bytes;  // instrumentation: the pass's algorithmic bytes (nullptr: off)
 };
 
@@ -891,9 +887,9 @@ __global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) 
         for (int f = f_lo; f < f_hi; ++f) {
           const bool is_min =
               a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-          if (box) run_stage<T, kOpSum, P, PP>(Vb, R, tot, n, TS, q, LS);
-          else if (is_min) run_stage<T, kOpMinK, P, PP>(Vb, R, tot, n, TS, q, LS);
-          else run_stage<T, kOpMaxK, P, PP>(Vb, R, tot, n, TS, q, LS);
+          if (box) run_stage<T, kOpSum, P, PP>(Vb, R, tot, n, TS, q, LS, a.seq_share);
+          else if (is_min) run_stage<T, kOpMinK, P, PP>(Vb, R, tot, n, TS, q, LS, a.seq_share);
+          else run_stage<T, kOpMaxK, P, PP>(Vb, R, tot, n, TS, q, LS, a.seq_share);
           store(cur, j_begin + jj, f, fac);
           if (a.bytes && threadIdx.x == 0) acct += static_cast<unsigned long long>(valid) * n * sizeof(T);
           __syncthreads();  // the next stage rewrites R and tot
@@ -955,9 +951,9 @@ __global__ void __launch_bounds__(kThreads) cube_long(Geom g, PassArgs<T> a, con
   for (int f = 0; f < nf; ++f) {
     T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
     const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-    if (box) run_stage<T, kOpSum, 1, 1>(V, R, tot, n, TS, q, 0);
-    else if (is_min) run_stage<T, kOpMinK, 1, 1>(V, R, tot, n, TS, q, 0);
-    else run_stage<T, kOpMaxK, 1, 1>(V, R, tot, n, TS, q, 0);
+    if (box) run_stage<T, kOpSum, 1, 1>(V, R, tot, n, TS, q, 0, a.seq_share);
+    else if (is_min) run_stage<T, kOpMinK, 1, 1>(V, R, tot, n, TS, q, 0, a.seq_share);
+    else run_stage<T, kOpMaxK, 1, 1>(V, R, tot, n, TS, q, 0, a.seq_share);
     // the epilogue in place (run_stage ended on a barrier: every output is written); pads are 0
     const T* aux = detsq ? a.aux + b * g.field : nullptr;
     for (int32_t i = threadIdx.x; i < static_cast<int32_t>(g.pitch); i += blockDim.x) {
@@ -1076,11 +1072,17 @@ template <class T>
 void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   const DevFacts f = dev_facts();
   const bool rows = a.axis == g.dim - 1;
+  const CubeTune tune = cube_tune_for(g, a.axis, sizeof(T));
+  a.seq_share = tune.seq_share > 0 ? tune.seq_share : kSeqShare;
   if (rows && smem_bytes(g.n[a.axis], 1, true, sizeof(T)) > f.smem) {
     launch_long<T>(s, g, a);
     return;
   }
-  const int P = lines_per_cta<T>(g, a.axis, f.smem);
+  int P = lines_per_cta<T>(g, a.axis, f.smem);
+  if (tune.lines > 0 && tune.lines <= 8 && smem_bytes(g.n[a.axis], tune.lines, rows, sizeof(T)) <= f.smem &&
+      (!rows || tune.lines <= std::max<int64_t>(1, g.rows))) {
+    P = tune.lines;
+  }
   if (a.rungs > kMaxRungs) throw std::invalid_argument("edab: more rungs than a cube launch holds");
   int64_t groups;
   if (rows) {
@@ -1096,16 +1098,11 @@ void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   const int64_t slots = static_cast<int64_t>(f.sms) * std::max<int64_t>(1, static_cast<int64_t>(f.sm_smem / (smem + 3072)));
   const int64_t resident = std::min<int64_t>(slots, static_cast<int64_t>(f.sms) * 4);
   const int64_t zc = a.rung_loop ? 1 : a.rungs;
-  int gpc = 1;
-  double best = 0.0;
-  for (int c = 1; c <= kMaxGroupsPerCta; ++c) {
-    const int64_t ctas = (groups + c - 1) / c * g.batch * zc;
-    const double cost = static_cast<double>((ctas + resident - 1) / resident) * (c + 1);
-    if (c == 1 || cost <= best) {
-      best = cost;
-      gpc = c;
-    }
-  }
+  // line groups per CTA: the tuned value, else one (measured fastest on the default shapes)
+  (void)resident;
+  (void)zc;
+  int gpc = tune.groups > 0 ? std::min(tune.groups, kMaxGroupsPerCta) : 1;
+  gpc = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(gpc, groups)));
   const int64_t gx = (groups + gpc - 1) / gpc;
   if (gx > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: cube launch too large");
   a.groups = groups;

@@ -382,6 +382,17 @@ template <class T>
 void cube(cudaStream_t s, const Geom& g, CubeOp op, const CubeArgs<T>& a);
 template <class T>
 void cube_simple(cudaStream_t s, const Geom& g, CubeOp op, const T* in, T* out0, T* out1, const int32_t* win);
+// The launch shape of a cube pass: lines per CTA (1, 2, 4 or 8), line groups per CTA, and the
+// segment share from which a window folds whole segments per worker; 0 leaves the default. The
+// shapes change no bit of any result (the folds are canonical): tune.cu times them per geometry
+// and keeps the fastest (eda_autotune); cube_tune_for returns the recorded shape of a pass, or the
+// calling thread's override while tuning.
+struct CubeTune {
+  int32_t lines = 0, groups = 0, seq_share = 0;
+};
+CubeTune cube_tune_for(const Geom& g, int axis, size_t es);
+void cube_tune_override(const CubeTune* t);  // nullptr: none (per calling thread)
+
 // 1-D lines too long for a pass to stage in shared memory fold in global memory: the calling host
 // thread provides a scratch of long_line_scratch_bytes (batch x pitch samples; 0 when the lines
 // fit) for the lines' fold input, before its cube calls.

@@ -7,6 +7,8 @@ it, and there is no CPU fallback."""
 from __future__ import annotations
 
 import operator
+
+import numpy as np
 from typing import Any
 
 from . import _native
@@ -29,6 +31,8 @@ __all__ = [
     "decompose_ragged",
     "device_count",
     "device_info",
+    "autotune",
+    "load_tuning",
     "monogenic",
     "set_transform_precision",
     "transform_precision",
@@ -75,3 +79,23 @@ def device_info(device: int = 0) -> dict[str, Any]:
     if not -(2**31) <= number < 2**31:
         raise ValueError(f"eda: CUDA device {number} is not visible")
     return _native.core().device_info(number)
+
+
+
+def autotune(shape: Any, batch: int = 1, dtype: Any = "float32", cache: str | None = None) -> dict[str, Any]:
+    """Times the launch shapes of the cube passes for fields of ``shape`` (1 to 3 axes) in batches of
+    ``batch`` on the current device and keeps the fastest for every later call with that geometry
+    (the results do not change, only the speed); with ``cache``, all kept shapes are written to that
+    file, which ``load_tuning`` (or the environment variable EDA_TUNING_CACHE) reads in a later
+    process. Returns the chosen shape and the timings (microseconds, default and tuned). This
+    engine's addition: the reference's launch shapes are fixed."""
+    dims = tuple(operator.index(v) for v in (shape if isinstance(shape, (tuple, list)) else (shape,)))
+    name = np.dtype(dtype).name if not isinstance(dtype, str) else dtype
+    if name not in ("float32", "float64"):
+        raise ValueError(f"eda: autotune dtype must be float32 or float64, got {dtype!r}")
+    return _native.core().autotune(name, dims, operator.index(batch), cache)
+
+
+def load_tuning(path: str) -> None:
+    """Reads launch shapes saved by ``autotune(..., cache=path)``."""
+    _native.core().tuning_load(path)

@@ -86,6 +86,11 @@ class Core:
                                         ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(vp)]
         L.eda_copy_to_host.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_int]
         L.eda_pointer_device.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        L.eda_autotune.argtypes = [ctypes.c_int, ctypes.c_int, i64, ctypes.POINTER(i64), ctypes.c_char_p,
+                                   ctypes.c_char_p, ctypes.c_size_t]
+        L.eda_tuning_load.argtypes = [ctypes.c_char_p]
+        L.eda_tuning_dump.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        L.eda_tuning_clear.argtypes = []
         self._lib = L
         self.path = str(path)
 
@@ -114,6 +119,26 @@ class Core:
         d = ctypes.c_int()
         self._check(self._lib.eda_pointer_device(ctypes.c_void_p(ptr), ctypes.byref(d)))
         return int(d.value)
+
+    # -- the cube passes' autotuner ------------------------------------------------------------
+    def autotune(self, dtype: str, shape: tuple[int, ...], batch: int, cache: str | None) -> dict:
+        n = (ctypes.c_int64 * 3)(*[int(v) for v in shape], *([1] * (3 - len(shape))))
+        buf = ctypes.create_string_buffer(1024)
+        code = 0 if np.dtype(dtype) == np.float32 else 1
+        self._check(self._lib.eda_autotune(code, len(shape), int(batch), n,
+                                           None if cache is None else str(cache).encode(), buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def tuning_load(self, path: str) -> None:
+        self._check(self._lib.eda_tuning_load(str(path).encode()))
+
+    def tuning_dump(self) -> str:
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.eda_tuning_dump(buf, len(buf)))
+        return buf.value.decode()
+
+    def tuning_clear(self) -> None:
+        self._check(self._lib.eda_tuning_clear())
 
     # -- the float32 transforms' product ------------------------------------------------------
     def set_transform_precision(self, mode: int) -> None:

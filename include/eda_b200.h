@@ -193,6 +193,21 @@ EDA_API int eda_buffer_dlpack(eda_buffer* b, size_t byte_offset, int dtype_code,
 EDA_API int eda_copy_to_host(void* dst, const void* src, size_t bytes, int device);
 EDA_API int eda_pointer_device(const void* p, int* device);
 
+/* The cube passes' autotuner (no counterpart in the reference, whose launch shapes are fixed,
+ * cpp/src/field/vhgw.cu:540-559). eda_autotune times the candidate launch shapes of the cube passes
+ * (lines per CTA, line groups per CTA, the segment share from which windows fold whole segments)
+ * on a synthetic field of the geometry (dtype, dim, batch, n) on the current device, records the
+ * fastest for that geometry (results are bit-identical under every shape) and, with cache_path,
+ * writes every record to that text file; report receives a JSON summary. eda_tuning_load reads a
+ * cache file into the records (the environment variable EDA_TUNING_CACHE names one that the first
+ * cube pass of the process loads); eda_tuning_dump writes the records as text; eda_tuning_clear
+ * forgets them. */
+EDA_API int eda_autotune(int dtype, int dim, int64_t batch, const int64_t* n, const char* cache_path, char* report,
+                         size_t len);
+EDA_API int eda_tuning_load(const char* cache_path);
+EDA_API int eda_tuning_dump(char* buf, size_t len);
+EDA_API int eda_tuning_clear(void);
+
 /* The product of the float32 orientation transforms, process-wide (no counterpart in the reference,
  * whose transforms are cuFFT's float32 FFTs, cpp/src/method/orientation.cu:674-767): 0 = 3xTF32
  * split products on the tensor cores (the default), 1 = BF16x3 split products on the tensor cores,

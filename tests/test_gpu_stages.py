@@ -275,3 +275,41 @@ def test_transform_precision_rejects_unknown_modes(dev):
     lib.eda_set_transform_precision.argtypes = [ctypes.c_int]
     assert lib.eda_set_transform_precision(3) == 1
     assert lib.eda_set_transform_precision(-1) == 1
+
+
+# Every launch shape the autotuner may choose gives the same bits: the cube filter under recorded
+# shapes (lines per CTA, groups per CTA, segment share) against the oracle, then a tuned geometry's
+# decomposition against the untuned one.
+@pytest.mark.parametrize("lines,groups,share", [(2, 1, 2), (4, 2, 8), (8, 2, 2), (8, 1, 64)])
+def test_cube_under_every_launch_shape(dev, tmp_path, lines, groups, share):
+    import eda
+
+    core = eda._native.core()
+    shape = (48, 200)
+    path = tmp_path / "tune.txt"
+    path.write_text("".join(f"4 2 {shape[0]} {shape[1]} 1 {bucket} {lines} {groups} {share} 1 1\n" for bucket in range(4)))
+    core.tuning_clear()
+    core.tuning_load(str(path))
+    try:
+        check(dev, shape, "maxmin", [1, 5, 33, 63, 129], np.float32)
+        check(dev, shape, "box", [3, 47, 95, 255], np.float32)
+        check(dev, shape, "maxmin", np.stack([[7, 41, 99], [65, 0, 13]]), np.float32, seed=5)
+    finally:
+        core.tuning_clear()
+
+
+def test_autotuned_geometry_decomposes_identically(dev, tmp_path):
+    import eda
+
+    rng = np.random.default_rng(4)
+    yy, xx = np.mgrid[0:96, 0:120]
+    x = np.stack([np.cos(2 * np.pi * (xx + k * yy) / 11) + 0.2 * rng.standard_normal((96, 120)) for k in (0.2, 0.5)])
+    x = x.astype(np.float32)
+    eda._native.core().tuning_clear()
+    want, want_info = eda.decompose(x, axes=(1, 2), return_info=True)
+    report = eda.autotune((96, 120), batch=2, cache=str(tmp_path / "t.txt"))
+    assert report["us_best"] <= report["us_default"]
+    got, info = eda.decompose(x, axes=(1, 2), return_info=True)
+    assert np.array_equal(got, want) and np.array_equal(info.windows, want_info.windows)
+    assert (tmp_path / "t.txt").read_text().count("\n") >= 2
+    eda._native.core().tuning_clear()
