@@ -215,6 +215,10 @@ def run_ours(args) -> None:
             pg.barrier()
         torch.cuda.synchronize(dev)
 
+    # the cube passes' launch shapes for this geometry (the autotuner; outside the timed region)
+    tuned = None if args.no_tune else eda.autotune((SIDE, SIDE), batch=batch)
+    # the clock sampler starts before the warm-up, so that its start-up stays out of the timed steps
+    clk = Clocks(local).__enter__()
     # warm-up (device input)
     for _ in range(args.warmup):
         eda.decompose(x_dev, axes=(1, 2))
@@ -222,7 +226,7 @@ def run_ours(args) -> None:
     # timed: device-resident inputs, events around each call, L2 flushed between calls
     lib.eda_profile(1)
     ms = []
-    with Clocks(local) as clk:
+    try:
         for _ in range(args.steps):
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -231,6 +235,8 @@ def run_ours(args) -> None:
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+    finally:
+        clk.__exit__(None, None, None)
     launches, cl, cb, cms = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
     lib.eda_profile_read(ctypes.byref(launches), ctypes.byref(cl), ctypes.byref(cb), ctypes.byref(cms))
     lib.eda_profile(0)
@@ -298,7 +304,8 @@ def run_ours(args) -> None:
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"2-D {batch} x {SIDE}x{SIDE} float32 images per GPU (rings, wavy stripes, blobs, "
                                "noise), sifts 3", "l2": "flushed between steps (256 MiB write)",
-                   "rows_per_element": int(P), "parallelism": f"replicas x{world}"},
+                   "rows_per_element": int(P), "parallelism": f"replicas x{world}",
+                   "cube_launch_shape": tuned},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "cube_pass", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
@@ -458,11 +465,14 @@ def run_other(args) -> None:
         call_host = lambda: eda.decompose(data, axes=axes)  # noqa: E731
         h2d = data.nbytes
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    if not args.no_tune and not ragged:
+        eda.autotune(data.shape[1:], batch=data.shape[0])
+    clk = Clocks(0).__enter__()  # started before the warm-up (its start-up stays out of the timed steps)
     for _ in range(args.warmup):
         call_dev()
     torch.cuda.synchronize(dev)
     ms = []
-    with Clocks(0) as clk:
+    try:
         for _ in range(args.steps):
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -471,6 +481,8 @@ def run_other(args) -> None:
             e1.record()
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+    finally:
+        clk.__exit__(None, None, None)
     for _ in range(args.warmup):
         call_host()
     wall, d2h = [], 0
@@ -565,6 +577,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling runs)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the cube passes' default launch shapes (no autotuning before the warm-up)")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="images per GPU of the 2-D benchmark (64; smaller only for profiling captures)")
     ap.add_argument("--workload", default="2d", choices=("2d", "1d", "3d", "ragged1d", "ragged1d-short", "ragged2d"),
