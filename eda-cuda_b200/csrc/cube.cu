@@ -585,6 +585,7 @@ struct PassArgs {
   int64_t groups;         // line groups per element
   int32_t gpc;            // line groups per CTA (blockIdx.x runs groups [x gpc, x gpc + gpc))
   int32_t seq_share;      // windows of at least workers / seq_share segments fold whole segments
+  int32_t dbuf;           // two staging buffers (a CTA that stages more than once copies ahead)
   unsigned long long* bytes;  // instrumentation: the pass's algorithmic bytes (nullptr: off)
 };
 
@@ -650,7 +651,10 @@ struct Vec16<double> {
 };
 
 template <class T, int P, bool ROWS>
-__global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) {
+#ifndef EDAB_CUBE_CTAS
+#define EDAB_CUBE_CTAS 4
+#endif
+__global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, PassArgs<T> a) {
   constexpr int VW = 16 / static_cast<int>(sizeof(T));  // samples per 16-byte copy
   constexpr int PP = ROWS ? 1 : P;                        // sample stride in shared memory
   using V16 = typename Vec16<T>::type;
@@ -668,7 +672,7 @@ __global__ void __launch_bounds__(kThreads, 4) cube_pass(Geom g, PassArgs<T> a) 
   const int32_t LS = ROWS ? row_stride<T>(n) : 1;  // line stride in shared memory
   const int32_t gel = group_elems<T>(n, P, ROWS);
   T* V0 = reinterpret_cast<T*>(smem_raw);
-  T* V1 = V0 + gel;
+  T* V1 = a.dbuf ? V0 + gel : V0;  // a CTA that stages once keeps one staging buffer
   T* R = V1 + gel;
   T* tot = R + gel;
   const int32_t j_begin = a.rung_loop ? 0 : static_cast<int32_t>(blockIdx.z);
@@ -981,9 +985,9 @@ __global__ void __launch_bounds__(kThreads) cube_long(Geom g, PassArgs<T> a, con
 thread_local void* t_long_scratch = nullptr;
 thread_local size_t t_long_bytes = 0;
 
-size_t smem_bytes(int32_t n, int P, bool rows, size_t es) {
+size_t smem_bytes(int32_t n, int P, bool rows, size_t es, bool dbuf = true) {
   const int32_t gel = es == 4 ? group_elems<float>(n, P, rows) : group_elems<double>(n, P, rows);
-  return (static_cast<size_t>(3) * gel + static_cast<size_t>(2) * tot_slots(n) * P) * es;
+  return (static_cast<size_t>(dbuf ? 3 : 2) * gel + static_cast<size_t>(2) * tot_slots(n) * P) * es;
 }
 
 template <class T>
@@ -1092,17 +1096,15 @@ void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
     for (int ax = 0; ax < a.axis; ++ax) outer *= g.n[ax];
     groups = outer * (g.stride[a.axis] / P);
   }
-  const size_t smem = smem_bytes(g.n[a.axis], P, rows, sizeof(T));
-  // line groups per CTA: the fewest waves of CTAs times the groups a CTA runs (plus one for its
-  // setup and the first copy), more groups per CTA on a tie
-  const int64_t slots = static_cast<int64_t>(f.sms) * std::max<int64_t>(1, static_cast<int64_t>(f.sm_smem / (smem + 3072)));
-  const int64_t resident = std::min<int64_t>(slots, static_cast<int64_t>(f.sms) * 4);
-  const int64_t zc = a.rung_loop ? 1 : a.rungs;
   // line groups per CTA: the tuned value, else one (measured fastest on the default shapes)
-  (void)resident;
-  (void)zc;
   int gpc = tune.groups > 0 ? std::min(tune.groups, kMaxGroupsPerCta) : 1;
   gpc = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(gpc, groups)));
+  // a second staging buffer only for a CTA that stages more than once (several groups, or the two
+  // fields of a max+min pass with separate inputs)
+  const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
+  const bool shared_in = a.in_stride == 0 && (nf == 1 || a.in1 == nullptr);
+  a.dbuf = (gpc > 1 || (shared_in ? 1 : nf) > 1) ? 1 : 0;
+  const size_t smem = smem_bytes(g.n[a.axis], P, rows, sizeof(T), a.dbuf != 0);
   const int64_t gx = (groups + gpc - 1) / gpc;
   if (gx > 0x7fffffffLL || g.batch > 65535) throw std::invalid_argument("edab: cube launch too large");
   a.groups = groups;
