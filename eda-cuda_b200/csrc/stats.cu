@@ -234,6 +234,16 @@ __device__ __forceinline__ bool sel_key_of(const Geom& g, const SelView<T>& a, i
   return true;
 }
 
+// One shared-memory count per distinct digit among the warp's active lanes (the lanes holding the
+// same digit add together through their lowest lane): a field's items crowd into few digit values
+// (the sign and exponent bits lead every key), and per-lane atomics on one address serialize.
+__device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t digit, bool take) {
+  const unsigned active = __ballot_sync(0xffffffffu, take);
+  if (!take) return;
+  const unsigned same = __match_any_sync(active, digit);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[digit], static_cast<uint32_t>(__popc(same)));
+}
+
 template <class K>
 struct SelLeader {
   K prefix[2];
@@ -341,17 +351,16 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
     const bool two = pass > 0 && !L->same;
     const K p0 = L->prefix[0], p1 = L->prefix[1];
     const int64_t stride = static_cast<int64_t>(ctas) * kThreads;
-    for (int64_t t = static_cast<int64_t>(me) * kThreads + tid; t < a.items; t += stride) {
-      K k;
-      if (!sel_key_of<T, K>(g, a, b, t, &k)) continue;
+    // the warp steps through the items together (count_digit is warp-collective)
+    const int64_t t_end = (a.items + 31) / 32 * 32;
+    for (int64_t t = static_cast<int64_t>(me) * kThreads + tid; t < t_end + stride; t += stride) {
+      if (t - tid % 32 >= a.items) break;  // the warp's first item is past the end: the whole warp leaves
+      K k = K(0);
+      const bool have = t < a.items && sel_key_of<T, K>(g, a, b, t, &k);
       const uint32_t digit = static_cast<uint32_t>((k >> shift) & dmask);
-      if (pass == 0) {
-        atomicAdd(&local[digit], 1u);
-        continue;
-      }
-      const K top = k >> hi;
-      if (top == (p0 >> hi)) atomicAdd(&local[digit], 1u);
-      if (two && top == (p1 >> hi)) atomicAdd(&local[kDigitBins + digit], 1u);
+      const K top = pass == 0 ? K(0) : (k >> hi);
+      count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
+      if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
     }
     __syncthreads();
     const int bins = 1 << width;
@@ -415,6 +424,141 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
   }
 }
 
+// The grid-wide form for batches too small to fill the GPU with clusters (few, large elements):
+// per digit, a counting launch over many CTAs per element (warp-aggregated shared-memory counts,
+// flushed with one global atomic per digit value and CTA) and a pick launch of one CTA per element
+// (the same block-wide prefix sum), the element's state in global memory between launches.
+template <class K>
+struct SelGridState {
+  K prefix[2];
+  unsigned long long rank[2];
+  long long count;
+  double gamma;
+  int32_t live, same;
+};
+
+template <int KeyBits>
+__device__ __forceinline__ void digit_of_pass(int pass, int* hi, int* shift, int* width) {
+  *hi = KeyBits - kDigitBits * pass;
+  *shift = *hi > kDigitBits ? *hi - kDigitBits : 0;
+  *width = *hi - *shift;
+}
+
+template <class T, class K>
+__global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T> a, const int32_t* run,
+                                                             const SelGridState<K>* st,
+                                                             unsigned long long* table, int32_t pass) {
+  __shared__ uint32_t local[2 * kDigitBins];
+  const int64_t b = blockIdx.y;
+  if (run && !run[b]) return;
+  bool two = false;
+  K p0 = K(0), p1 = K(0);
+  if (pass > 0) {
+    if (!st[b].live) return;
+    two = !st[b].same;
+    p0 = st[b].prefix[0];
+    p1 = st[b].prefix[1];
+  }
+  int hi, shift, width;
+  digit_of_pass<8 * static_cast<int>(sizeof(K))>(pass, &hi, &shift, &width);
+  const K dmask = static_cast<K>((K(1) << width) - K(1));
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 2 * kDigitBins; i += kThreads) local[i] = 0u;
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * kThreads;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * kThreads + tid;; t += stride) {
+    if (t - tid % 32 >= a.items) break;  // the warp's first item is past the end
+    K k = K(0);
+    const bool have = t < a.items && sel_key_of<T, K>(g, a, b, t, &k);
+    const uint32_t digit = static_cast<uint32_t>((k >> shift) & dmask);
+    const K top = pass == 0 ? K(0) : (k >> hi);
+    count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
+    if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
+  }
+  __syncthreads();
+  const int bins = 1 << width;
+  unsigned long long* tb = table + static_cast<int64_t>(b) * 2 * kDigitBins;
+  for (int i = tid; i < (two ? 2 : 1) * bins; i += kThreads) {
+    const int r = i >= bins ? 1 : 0;
+    const uint32_t c = local[r * kDigitBins + (i - r * bins)];
+    if (c) atomicAdd(&tb[r * kDigitBins + (i - r * bins)], static_cast<unsigned long long>(c));
+  }
+}
+
+template <class K>
+__global__ void __launch_bounds__(kThreads) select_grid_pick(const int32_t* run, SelGridState<K>* st,
+                                                            unsigned long long* table, int32_t pass, double q,
+                                                            double* out, int64_t* count_out) {
+  constexpr int kKeyBits = 8 * static_cast<int>(sizeof(K));
+  constexpr int kDigits = (kKeyBits + kDigitBits - 1) / kDigitBits;
+  __shared__ SelGridState<K> S;
+  __shared__ unsigned long long warp_tot[kThreads / 32];
+  __shared__ int hit_bin;
+  __shared__ unsigned long long hit_rest;
+  const int64_t b = blockIdx.x;
+  if (run && !run[b]) return;
+  const int tid = threadIdx.x;
+  int hi, shift, width;
+  digit_of_pass<kKeyBits>(pass, &hi, &shift, &width);
+  const int bins = 1 << width;
+  unsigned long long* tb = table + static_cast<int64_t>(b) * 2 * kDigitBins;
+  if (pass == 0) {
+    unsigned long long n = 0;
+    for (int i = tid; i < bins; i += kThreads) n += tb[i];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) n += __shfl_xor_sync(0xffffffffu, n, d);
+    if ((tid & 31) == 0) warp_tot[tid >> 5] = n;
+    __syncthreads();
+    if (tid == 0) {
+      unsigned long long total = 0;
+      for (int w = 0; w < kThreads / 32; ++w) total += warp_tot[w];
+      S.prefix[0] = S.prefix[1] = K(0);
+      S.same = 1;
+      S.count = static_cast<long long>(total);
+      S.live = total > 0;
+      S.gamma = 0.0;
+      if (q < 0) {
+        S.rank[0] = total ? (total - 1) / 2 : 0;
+        S.rank[1] = total / 2;
+      } else if (total) {
+        long long i = 0, j = 0;
+        linear_index(static_cast<long long>(total), q, &i, &j, &S.gamma);
+        S.rank[0] = static_cast<unsigned long long>(i);
+        S.rank[1] = static_cast<unsigned long long>(j);
+      }
+    }
+  } else if (tid == 0) {
+    S = st[b];
+  }
+  __syncthreads();
+  const bool two = pass > 0 && !S.same;
+  if (S.live) {
+    for (int r = 0; r < 2; ++r) {
+      rank_digit(tb + (two ? r : 0) * kDigitBins, bins, S.rank[r], warp_tot, &hit_bin, &hit_rest);
+      if (tid == 0) {
+        S.prefix[r] |= static_cast<K>(hit_bin) << shift;
+        S.rank[r] = hit_rest;
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < 2 * kDigitBins; i += kThreads) tb[i] = 0ULL;  // clean for the next digit
+  if (tid == 0) {
+    S.same = S.prefix[0] == S.prefix[1];
+    st[b] = S;
+    if (pass == kDigits - 1) {
+      if (!S.live) {
+        out[b] = d_nan();
+        if (count_out) count_out[b] = 0;
+      } else {
+        const double v0 = key_value(S.prefix[0]), v1 = key_value(S.prefix[1]);
+        out[b] = q < 0 ? ((S.count & 1) ? v0 : __dmul_rn(__dadd_rn(v0, v1), 0.5)) : linear_between(v0, v1, S.gamma);
+        if (count_out) count_out[b] = S.count;
+      }
+    }
+  }
+}
+
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 }  // namespace
@@ -437,11 +581,34 @@ void field_totals(cudaStream_t s, const Geom& g, const T* f, double* energy, dou
   EDAB_LAUNCH("element_totals");
 }
 
-size_t select_scratch_bytes(const Geom&) { return 0; }
+size_t select_scratch_bytes(const Geom& g) {
+  return align256(static_cast<size_t>(g.batch) * sizeof(SelGridState<uint64_t>)) +
+         align256(static_cast<size_t>(g.batch) * 2 * kDigitBins * sizeof(unsigned long long));
+}
+
+// The grid-wide form: every digit a counting and a pick launch (scratch: the states, then the
+// [B][2][bins] count tables, zeroed here and left zeroed by every pick).
+template <class T, class K>
+void select_grid(cudaStream_t s, const Geom& g, const SelView<T>& a, double q, const int32_t* run, double* out,
+                 int64_t* count, void* scratch) {
+  constexpr int kDigits = (8 * static_cast<int>(sizeof(K)) + kDigitBits - 1) / kDigitBits;
+  auto* st = static_cast<SelGridState<K>*>(scratch);
+  auto* table = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) +
+                                                       align256(static_cast<size_t>(g.batch) * sizeof(SelGridState<uint64_t>)));
+  EDAB_CUDA(cudaMemsetAsync(table, 0, static_cast<size_t>(g.batch) * 2 * kDigitBins * sizeof(unsigned long long), s));
+  const int64_t per_cta = int64_t{kThreads} * 64;
+  const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>((a.items + per_cta - 1) / per_cta, 1, 1024));
+  for (int pass = 0; pass < kDigits; ++pass) {
+    select_grid_count<T, K><<<dim3(ctas, static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(g, a, run, st, table, pass);
+    EDAB_LAUNCH("select_grid_count");
+    select_grid_pick<K><<<static_cast<unsigned>(g.batch), kThreads, 0, s>>>(run, st, table, pass, q, out, count);
+    EDAB_LAUNCH("select_grid_pick");
+  }
+}
 
 template <class T>
 void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const int32_t* run, double* out,
-            int64_t* count, void*) {
+            int64_t* count, void* scratch) {
   SelView<T> a{};
   a.sel = sel;
   if (sel.src == SelSrc::kField) {
@@ -454,6 +621,24 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
     a.items = static_cast<int64_t>(a.naxes) * g.field;
   }
   if (g.batch > 65535) throw std::invalid_argument("edab: select batch too large");
+  // clusters (one launch) when the batch fills the GPU with them, else the grid-wide form
+  int sms = 148;
+  {
+    int dev = 0;
+    EDAB_CUDA(cudaGetDevice(&dev));
+    EDAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  if (g.batch * kSelClusterMax < 2 * static_cast<int64_t>(sms)) {
+    if (!scratch) throw std::logic_error("edab: the grid-wide selection needs its scratch");
+    if constexpr (std::is_same_v<T, float>) {
+      if (sel.center == nullptr) {
+        select_grid<T, uint32_t>(s, g, a, q, run, out, count, scratch);
+        return;
+      }
+    }
+    select_grid<T, uint64_t>(s, g, a, q, run, out, count, scratch);
+    return;
+  }
   // CTAs per element: about 16 items per thread, up to a cluster of 8
   const int64_t per_cta = int64_t{kThreads} * 16;
   const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>((a.items + per_cta - 1) / per_cta, 1, kSelClusterMax));

@@ -160,7 +160,9 @@ void run_select(const void* x_dev, int dim, int64_t batch, const int64_t* n, int
   sel.bits = static_cast<uint8_t>(bits);
   sel.axes = static_cast<uint8_t>(axes);
   sel.center = c;
-  select<T>(s, g, sel, q, nullptr, o, k, nullptr);
+  void* scratch = nullptr;
+  EDAB_CUDA(cudaMalloc(&scratch, select_scratch_bytes(g)));
+  select<T>(s, g, sel, q, nullptr, o, k, scratch);
   EDAB_CUDA(cudaMemcpyAsync(out, o, sizeof(double) * batch, cudaMemcpyDeviceToHost, s));
   if (count) EDAB_CUDA(cudaMemcpyAsync(count, k, sizeof(int64_t) * batch, cudaMemcpyDeviceToHost, s));
   EDAB_CUDA(cudaStreamSynchronize(s));
@@ -169,6 +171,7 @@ void run_select(const void* x_dev, int dim, int64_t batch, const int64_t* n, int
   cudaFree(c);
   cudaFree(o);
   cudaFree(k);
+  cudaFree(scratch);
 }
 
 template <class T>

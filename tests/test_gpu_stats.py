@@ -274,3 +274,23 @@ def test_components(dev, shape, density):
         for b in range(shape[0]):
             want = oracle.components((mask[b] & bits) != 0)
             assert np.array_equal(got[b].astype(np.int64), want)
+
+
+# Batches of 40 or more elements fill the GPU with clusters (one launch per selection); smaller
+# batches take the grid-wide form (a counting and a pick launch per digit): both forms, every kind.
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("shape", [(40, 300), (48, 32, 48), (40, 6, 7, 9)])
+def test_select_in_clusters(dev, dtype, shape):
+    x = field(shape, dtype, sum(shape), "ties")
+    rng = np.random.default_rng(1)
+    mask = rng.integers(0, 2, shape).astype(np.uint8)
+    center = rng.standard_normal(shape[0])
+    for kw in ({}, {"mask": mask}, {"center": center}, {"src": 1, "axes": 1}, {"src": 1, "axes": (1 << (len(shape) - 1)) - 1}):
+        for q in (-1.0, 0.25):
+            out, cnt = gpu_select(dev, x, q=q, **kw)
+            for b in range(shape[0]):
+                v = items(x[b], kw.get("src", 0), kw.get("axes", 0), None if "mask" not in kw else mask[b], 1,
+                          None if "center" not in kw else center[b])
+                want = oracle.select(v, q)
+                assert (np.isnan(out[b]) and np.isnan(want)) or out[b] == want, (kw, q, b)
+                assert cnt[b] == v.size
