@@ -216,7 +216,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize(dev)
 
     # the cube passes' launch shapes for this geometry (the autotuner; outside the timed region)
-    tuned = None if args.no_tune else eda.autotune((SIDE, SIDE), batch=batch)
+    tuned = eda.autotune((SIDE, SIDE), batch=batch) if args.tune else None
     # the clock sampler starts before the warm-up, so that its start-up stays out of the timed steps
     clk = Clocks(local).__enter__()
     # warm-up (device input)
@@ -465,7 +465,7 @@ def run_other(args) -> None:
         call_host = lambda: eda.decompose(data, axes=axes)  # noqa: E731
         h2d = data.nbytes
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
-    if not args.no_tune and not ragged:
+    if args.tune and not ragged:
         eda.autotune(data.shape[1:], batch=data.shape[0])
     clk = Clocks(0).__enter__()  # started before the warm-up (its start-up stays out of the timed steps)
     for _ in range(args.warmup):
@@ -577,8 +577,9 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling runs)")
-    ap.add_argument("--no-tune", action="store_true",
-                    help="keep the cube passes' default launch shapes (no autotuning before the warm-up)")
+    ap.add_argument("--tune", action="store_true",
+                    help="autotune the cube passes' launch shapes for the workload's geometry before the warm-up "
+                         "(on the 2-D workload the tuner keeps the default shape)")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="images per GPU of the 2-D benchmark (64; smaller only for profiling captures)")
     ap.add_argument("--workload", default="2d", choices=("2d", "1d", "3d", "ragged1d", "ragged1d-short", "ragged2d"),
