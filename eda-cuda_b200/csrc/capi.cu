@@ -313,4 +313,10 @@ int eda_set_transform_precision(int mode) {
 
 int eda_transform_precision(void) { return static_cast<int>(edab::transform_precision()); }
 
+int eda_set_length_classes(int32_t on) {
+  return guarded([&] { edab::set_length_classes(on != 0); });
+}
+
+int eda_length_classes(void) { return edab::length_classes() ? 1 : 0; }
+
 }  // extern "C"

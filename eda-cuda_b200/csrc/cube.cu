@@ -665,7 +665,7 @@ __global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, Pa
   const int64_t b = blockIdx.y;
   const int axis = a.axis;
   // (a kernel parameter indexed by a runtime value would be copied to local memory)
-  const int32_t n = geom_n(g, axis);
+  const int32_t n = elem_n(g, b, axis);
   const int64_t inner = ROWS ? 1 : geom_stride(g, axis);  // column panels: the axis stride
   const int64_t step = ROWS ? 1 : inner;
   const int32_t TS = tot_slots(n);
@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, Pa
         double prod = 1.0;
 #pragma unroll
         for (int ax = 0; ax < kMaxDim; ++ax) {
-          if (ax < g.dim) prod *= static_cast<double>(2 * min((w - 1) / 2, g.n[ax] - 1) + 1);
+          if (ax < g.dim) prod *= static_cast<double>(2 * min((w - 1) / 2, (g.len ? n : g.n[ax]) - 1) + 1);
         }
         fac_s[jj] = static_cast<T>(1.0 / prod);
       }
@@ -937,7 +937,7 @@ __global__ void __launch_bounds__(kThreads) cube_long(Geom g, PassArgs<T> a, con
   __shared__ T fac_s;
   const int64_t b = blockIdx.x;
   const int32_t j = static_cast<int32_t>(blockIdx.y);
-  const int32_t n = g.n_last;
+  const int32_t n = elem_len(g, b);
   const int32_t w = a.win[static_cast<int64_t>(j) * g.batch + b];
   if (w < 1) return;
   const bool box = a.op == static_cast<int>(CubeOp::kBox);

@@ -170,9 +170,12 @@ Run::~Run() {
 
 namespace {
 
+// dst (B, P, count) from the rows (B, cap, src_count): src_count > count for an element of a 1-D
+// batch of uneven lengths (its rows are laid out at the batch's longest length).
 template <class T>
-__global__ void collect_kernel(int64_t B, int32_t P, int32_t cap, int64_t count, const int32_t* n_imfs,
-                               const int32_t* error, const T* __restrict__ src, T* __restrict__ dst) {
+__global__ void collect_kernel(int64_t B, int32_t P, int32_t cap, int64_t count, int64_t src_count,
+                               const int32_t* n_imfs, const int32_t* error, const T* __restrict__ src,
+                               T* __restrict__ dst) {
   const int64_t total = B * P * count;
   for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
        idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -182,7 +185,7 @@ __global__ void collect_kernel(int64_t B, int32_t P, int32_t cap, int64_t count,
     const int64_t b = bk / P;
     T v;
     if (error[b] != 0) v = static_cast<T>(d_nan());
-    else if (k <= n_imfs[b]) v = src[(b * cap + k) * count + i];
+    else if (k <= n_imfs[b]) v = src[(b * cap + k) * src_count + i];
     else v = T(0);
     dst[idx] = v;
   }
@@ -219,6 +222,7 @@ int32_t max_axis(int dtype, int dim) { return dim == 1 ? kMaxLine1D : (dtype == 
 }  // namespace
 
 void Run::collect(void* dst, bool dst_on_device, cudaStream_t s) {
+  if (!lens.empty()) throw std::logic_error("eda: a batch of uneven lengths is collected element by element");
   if (batch == 0 || rows == 0) return;
   const size_t es = dtype == 0 ? 4 : 8;
   const size_t elems = static_cast<size_t>(batch) * rows * count;
@@ -231,10 +235,10 @@ void Run::collect(void* dst, bool dst_on_device, cudaStream_t s) {
   const unsigned blocks = blocks_for(static_cast<int64_t>(elems) / 4 + 1);
   const unsigned grid = std::min<unsigned>(blocks, 1u << 20);
   if (dtype == 0) {
-    collect_kernel<float><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, meta, meta + batch,
+    collect_kernel<float><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, count, meta, meta + batch,
                                                     static_cast<const float*>(dev_rows), static_cast<float*>(out));
   } else {
-    collect_kernel<double><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, meta, meta + batch,
+    collect_kernel<double><<<grid, kThreads, 0, s>>>(batch, rows, rows_cap, count, count, meta, meta + batch,
                                                      static_cast<const double*>(dev_rows), static_cast<double*>(out));
   }
   EDAB_LAUNCH("collect_kernel");
@@ -288,7 +292,8 @@ void Run::collect_one(int64_t j, void* dst, bool dst_on_device, cudaStream_t s) 
   if (j < 0 || j >= batch) throw std::invalid_argument("eda: element index out of range");
   const size_t es = dtype == 0 ? 4 : 8;
   const int32_t P = rows_of(j);
-  const size_t elems = static_cast<size_t>(P) * static_cast<size_t>(count);
+  const int64_t cj = count_of(j);
+  const size_t elems = static_cast<size_t>(P) * static_cast<size_t>(cj);
   int32_t* meta = nullptr;
   EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&meta), sizeof(int32_t) * 2, s));
   EDAB_CUDA(cudaMemcpyAsync(meta, n_imfs.data() + j, sizeof(int32_t), cudaMemcpyHostToDevice, s));
@@ -298,10 +303,10 @@ void Run::collect_one(int64_t j, void* dst, bool dst_on_device, cudaStream_t s) 
   const unsigned grid = std::min<unsigned>(blocks_for(static_cast<int64_t>(elems) / 4 + 1), 1u << 20);
   const size_t off = static_cast<size_t>(j) * static_cast<size_t>(rows_cap) * static_cast<size_t>(count);
   if (dtype == 0) {
-    collect_kernel<float><<<grid, kThreads, 0, s>>>(1, P, rows_cap, count, meta, meta + 1,
+    collect_kernel<float><<<grid, kThreads, 0, s>>>(1, P, rows_cap, cj, count, meta, meta + 1,
                                                     static_cast<const float*>(dev_rows) + off, static_cast<float*>(out));
   } else {
-    collect_kernel<double><<<grid, kThreads, 0, s>>>(1, P, rows_cap, count, meta, meta + 1,
+    collect_kernel<double><<<grid, kThreads, 0, s>>>(1, P, rows_cap, cj, count, meta, meta + 1,
                                                      static_cast<const double*>(dev_rows) + off,
                                                      static_cast<double*>(out));
   }
@@ -348,14 +353,30 @@ void validate(int dtype, int dim, int64_t batch, const int64_t* n, const Params&
 
 namespace {
 
-// decompose() and decompose_strided(): src (device input only) gives the input's own layout and
-// element type, converted chunk by chunk into the staging buffer; without it x is dense.
+// decompose(), decompose_strided() and decompose_lengths(): src (device input only) gives the
+// input's own layout and element type, converted chunk by chunk into the staging buffer; without it
+// x is dense. lens (host, 1-D only): every element's length, n[0] their maximum.
 std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceView* src, int dtype, int dim,
-                                    int64_t batch, const int64_t* n, const Params& p, cudaStream_t s) {
+                                    int64_t batch, const int64_t* n, const Params& p, cudaStream_t s,
+                                    const int32_t* lens = nullptr) {
   validate(dtype, dim, batch, n, p);
   const bool f32 = dtype == 0;
   const size_t es = f32 ? 4 : 8;
   const Geom g = make_geom(dim, batch, n);
+  // the lengths on the device, released with the call
+  struct DeviceLens {
+    int32_t* p = nullptr;
+    cudaStream_t s = nullptr;
+    ~DeviceLens() {
+      if (p) cudaFreeAsync(p, s);
+    }
+  } dlens;
+  if (lens) {
+    if (dim != 1) throw std::invalid_argument("eda: uneven lengths are 1-D only");
+    dlens.s = s;
+    EDAB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&dlens.p), sizeof(int32_t) * static_cast<size_t>(batch), s));
+    EDAB_CUDA(cudaMemcpyAsync(dlens.p, lens, sizeof(int32_t) * static_cast<size_t>(batch), cudaMemcpyHostToDevice, s));
+  }
   const double tau = p.tie_tolerance >= 0 ? p.tie_tolerance : (f32 ? std::ldexp(1.0, -14) : std::ldexp(1.0, -30));
   Ctl c = make_ctl(g, f32, p.sifts, tau, p.max_imf, p.check_finite, 0);
   const int32_t bound = mode_bound(c);
@@ -368,6 +389,7 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
   run->geom = g;
   run->batch = batch;
   run->count = g.count;
+  if (lens) run->lens.assign(lens, lens + batch);
   run->rows_cap = cap;
   const size_t row_bytes = static_cast<size_t>(batch) * cap * static_cast<size_t>(g.count) * es;
   const size_t he = static_cast<size_t>(batch) * static_cast<size_t>(cap - 1);
@@ -420,7 +442,11 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
   std::vector<Elem> part;
   for (int64_t b0 = 0; b0 < batch; b0 += Bc) {
     const int64_t nb = std::min(Bc, batch - b0);
-    const Geom gc = make_geom(dim, nb, n);
+    Geom gc = make_geom(dim, nb, n);
+    if (lens) {
+      gc.len = dlens.p + b0;
+      gc.len_host = lens + b0;
+    }
     ws.reset();
     // the chunk's dense input, staged at the head of the workspace
     void* staged = ws.take<unsigned char>(static_cast<size_t>(nb) * static_cast<size_t>(g.count) * es);
@@ -496,6 +522,18 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
 std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
                                const Params& p, cudaStream_t s) {
   return decompose_impl(x, on_device, nullptr, dtype, dim, batch, n, p, s);
+}
+
+std::unique_ptr<Run> decompose_lengths(const void* x, bool on_device, int dtype, int64_t batch, const int32_t* lens,
+                                       const Params& p, cudaStream_t s) {
+  if (batch > 0 && (!x || !lens)) throw std::invalid_argument("eda: null argument");
+  int64_t n_max = 1;
+  for (int64_t b = 0; b < batch; ++b) {
+    const int64_t nb = lens[b];
+    validate(dtype, 1, 1, &nb, p);
+    n_max = std::max(n_max, nb);
+  }
+  return decompose_impl(x, on_device, nullptr, dtype, 1, batch, &n_max, p, s, lens);
 }
 
 std::unique_ptr<Run> decompose_strided(const void* x, const SourceView& src, int dtype, int dim, const int64_t* n,

@@ -90,6 +90,7 @@ struct Run {
   int32_t rows = 1, rows_cap = 0, K = 0;
   std::vector<int32_t> n_imfs, error, hist_scale, hist_sifts;
   std::vector<double> hist_spacing, hist_energy;
+  std::vector<int32_t> lens;  // a 1-D batch of uneven lengths: every element's length (else empty)
   void* dev_rows = nullptr;  // from the device's rows pool (rows_alloc)
   void* dev_orient = nullptr;  // (B, cap - 1, D + 1, count) with Params::orientation, rows pool
   ~Run();
@@ -101,11 +102,13 @@ struct Run {
   // elements (cpp/src/method/orientation.cu:524-549, eda_orientation_collect).
   void collect_orientation(void* dir, void* coh, bool dst_on_device, cudaStream_t s);
   int32_t rows_of(int64_t j) const { return error[static_cast<size_t>(j)] ? 1 : n_imfs[static_cast<size_t>(j)] + 1; }
+  // samples of element j (its length in a batch of uneven lengths)
+  int64_t count_of(int64_t j) const { return lens.empty() ? count : lens[static_cast<size_t>(j)]; }
 };
 
-// A ragged batch: elements of different shapes, decomposed in groups of equal shape (an element's
-// results do not depend on the batch around it) by concurrent workers, each with its own stream
-// and workspace.
+// A ragged batch: elements of different shapes, decomposed in groups (equal shapes, or 1-D length
+// classes run as batches of uneven lengths; an element's results do not depend on the batch around
+// it) by concurrent workers, each with its own stream and workspace.
 struct RaggedRun {
   int dtype = 0, dim = 1, device = 0;
   std::vector<std::unique_ptr<Run>> groups;
@@ -116,11 +119,19 @@ struct RaggedRun {
 // element on the current device, ready once `s` reaches the call. workers: concurrent groups (>= 1).
 std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_device, int dtype, int dim, int64_t count,
                                             const int64_t* n, const Params& p, int workers, cudaStream_t s);
+// 1-D ragged batches in length classes (on: the default) or by exact length (off), process-wide.
+void set_length_classes(bool on);
+bool length_classes();
 
 // Decomposes x (B, n_0..n_{D-1}), C-contiguous, float32 (dtype 0) or float64 (1), on the host or
 // the current device, on stream s. Throws std::invalid_argument, OutOfMemory or CudaError.
 std::unique_ptr<Run> decompose(const void* x, bool on_device, int dtype, int dim, int64_t batch, const int64_t* n,
                                const Params& p, cudaStream_t s);
+// Decomposes a 1-D batch of uneven lengths in one engine run: x (batch, max(lens)) holds element b
+// in its first lens[b] samples (the rest is not read). Element b's results are those of a call on
+// that element alone; collect them with Run::collect_one.
+std::unique_ptr<Run> decompose_lengths(const void* x, bool on_device, int dtype, int64_t batch, const int32_t* lens,
+                                       const Params& p, cudaStream_t s);
 
 // A device input read where it lies: element type (the C ABI's EDA_SRC_* codes), batch axes (C
 // order) and strides in elements of that type, of either sign.

@@ -65,6 +65,11 @@ void profile_cube_launch(cudaStream_t s, bool begin);
 // innermost axis padded to `pitch` (a multiple of 32: every row starts on a 128-byte boundary for
 // float, so rows load as whole sectors and as 16-byte vectors). Pad samples are zero and never
 // enter a result.
+//
+// A 1-D batch of uneven lengths (len != nullptr) lays every element out at the longest length
+// (n[0], pitch and count are the batch's longest) and gives element b its own length len[b]: every
+// kernel reads the element's extent through elem_len / elem_count, so an element's samples from
+// len[b] on are pads, and its results are those of a call on that element alone.
 struct Geom {
   int32_t dim;
   int32_t n[kMaxDim];       // n[a] = 1 for a >= dim
@@ -79,6 +84,8 @@ struct Geom {
   uint64_t pitch_inv;        // ceil(2^64 / pitch): v / pitch = umulhi(v, pitch_inv) for 0 <= v < 2^32
   uint64_t field_inv;        // ceil(2^64 / field): i / field = umulhi(i, field_inv) for 0 <= i < 2^64 / field
   int32_t field_fast;        // batch field^2 <= 2^64: every sample index of the batch divides by umulhi
+  const int32_t* len;        // 1-D batches of uneven lengths: element lengths (device), else nullptr
+  const int32_t* len_host;   // the same lengths in host memory (the host's per-element decisions)
 };
 Geom make_geom(int dim, int64_t batch, const int64_t* n);
 
@@ -99,6 +106,14 @@ __host__ __device__ inline int64_t pitch_row(const Geom& g, int64_t v) {
 }
 __host__ __device__ inline int64_t pitch_col(const Geom& g, int64_t v) { return v - pitch_row(g, v) * g.pitch; }
 __host__ __device__ inline bool is_pad(const Geom& g, int64_t v) { return pitch_col(g, v) >= g.n_last; }
+// The extent of element b along the last axis (its length in 1-D), and its sample count.
+__device__ __forceinline__ int32_t elem_len(const Geom& g, int64_t b) { return g.len ? __ldg(g.len + b) : g.n_last; }
+__device__ __forceinline__ int64_t elem_count(const Geom& g, int64_t b) { return g.len ? __ldg(g.len + b) : g.count; }
+// n[a] of element b (a ragged batch is 1-D: its only axis is the element's length).
+__device__ __forceinline__ int32_t elem_n(const Geom& g, int64_t b, int a) {
+  return g.len ? __ldg(g.len + b) : (a == 0 ? g.n[0] : (a == 1 ? g.n[1] : g.n[2]));
+}
+__device__ __forceinline__ bool is_pad_b(const Geom& g, int64_t b, int64_t v) { return pitch_col(g, v) >= elem_len(g, b); }
 // Element of sample index i of the batch (i / field without a 64-bit division where exact).
 __host__ __device__ inline int64_t elem_of(const Geom& g, int64_t i) {
 #ifdef __CUDA_ARCH__
@@ -131,11 +146,12 @@ __host__ __device__ inline bool voxel_coords(const Geom& g, int64_t v, int32_t* 
 }
 
 // voxel_coords for a compile-time D (the Geom parameter and x stay in registers).
+// nl: the element's extent along the last axis (elem_len).
 template <int D>
-__device__ __forceinline__ bool voxel_coords_d(const Geom& g, int64_t v, int32_t* x) {
+__device__ __forceinline__ bool voxel_coords_d(const Geom& g, int64_t v, int32_t nl, int32_t* x) {
   const int64_t row = pitch_row(g, v);
   const int64_t col = v - row * g.pitch;
-  if (col >= g.n[D - 1]) return false;
+  if (col >= nl) return false;
   x[D - 1] = static_cast<int32_t>(col);
   uint32_t q = static_cast<uint32_t>(row);  // row < field < 2^31
 #pragma unroll
@@ -313,9 +329,9 @@ inline unsigned blocks_for(int64_t n, int threads = kThreads) {
 // i = b * field + v.
 template <class Run, class F>
 __global__ void __launch_bounds__(kThreads) voxel_kernel(Geom g, Run run, F f) {
-  const int32_t nl = g.n_last;
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     if (!run(b)) continue;
+    const int32_t nl = elem_len(g, b);
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       if (pitch_col(g, v) >= nl) continue;

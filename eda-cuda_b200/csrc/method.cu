@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(kThreads) element_extent(Geom g, Ctl c, const 
   if (!run[b]) return;
   const T q = static_cast<T>(c.q), sm1 = static_cast<T>(c.span - 1.0);
   uint64_t lo_bits = ~0ULL, hi_bits = 0ULL;
-  const int32_t nl = g.n_last;
+  const int32_t nl = elem_len(g, b);
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field; v += step) {
     if (pitch_col(g, v) >= nl) continue;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kThreads) element_rungs(Geom g, uint8_t* lo, T
   const double w_first = static_cast<double>(el[b].rung_w[0]);
   const double w_last = static_cast<double>(el[b].rung_w[K > 0 ? K - 1 : 0]);
   unsigned used = 0u, pts = 0u;
-  const int32_t nl = g.n_last;
+  const int32_t nl = elem_len(g, b);
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field; v += step) {
     if (pitch_col(g, v) >= nl) continue;
@@ -401,16 +401,15 @@ __global__ void __launch_bounds__(kThreads, EDAB_GATHER_CTAS) gather_kernel(Geom
                                                          const T* __restrict__ o1, const T* __restrict__ o2,
                                                          const T* __restrict__ rung0, const T* __restrict__ rung1,
                                                          T* __restrict__ out0, T* __restrict__ out1) {
-  const int32_t nl = g.n_last;
   const int64_t fe = g.batch * g.field;
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     if (!run[b]) continue;
+    const int32_t nl = elem_len(g, b);
     const uint32_t pts_mask = el[b].rung_pts;
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       int32_t x[kMaxDim];
-      if (!voxel_coords_d<D>(g, v, x)) continue;
-      (void)nl;
+      if (!voxel_coords_d<D>(g, v, nl, x)) continue;
       const int64_t at = b * g.field + v;
       const int l = __ldg(lo + at);
       const T tt = __ldg(t + at);
@@ -479,10 +478,10 @@ template <class T, int D>
 __global__ void __launch_bounds__(kThreads) sift_step_kernel(Geom g, int32_t j, Elem* el, const T* __restrict__ r,
                                                             const T* __restrict__ h, const T* __restrict__ mh,
                                                             const T* __restrict__ a, T* __restrict__ hn) {
-  const int32_t nl = g.n_last;
   for (int64_t b = blockIdx.y; b < g.batch; b += gridDim.y) {
     const Elem& e = el[b];
     if (e.status != kActive || !e.sifting) continue;
+    const int32_t nl = elem_len(g, b);
     uint64_t m_res = 0, m_h = 0;
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -871,12 +870,13 @@ void Engine<T>::g2_test(const uint8_t* ff, uint8_t* P) {
   for_voxels(s_, g_, runS, [=] __device__(int64_t b, int64_t, int64_t i) {
     if (static_cast<double>(om[i]) > __dmul_rn(c.reset, p[b]) && t1[i] > T(0.5)) el[b].g2_any_jump = 1;
   });
+  const Geom g = g_;
   for_elements(s_, B_, [=] __device__(int64_t b) {
     if (srung[b] <= 0) return;
     Elem& e = el[b];
     e.g2_res_np = np[b];
     e.g2_res_p = p[b];
-    e.g2_res_cov = __ddiv_rn(static_cast<double>(np[b]), static_cast<double>(c.count));
+    e.g2_res_cov = __ddiv_rn(static_cast<double>(np[b]), static_cast<double>(elem_count(g, b)));
     if (np[b] == 0 || !e.g2_any_core) e.g2_res_outcome = kG2None;
     else if (__dmul_rn(c.fine_jump, p[b]) > static_cast<double>(e.w)) e.g2_res_outcome = kG2Stop;
     else e.g2_res_outcome = e.g2_any_jump ? kG2Accepted : kG2None;
@@ -1000,7 +1000,7 @@ void Engine<T>::g2() {
   for_samples(s_, B_ * g_.field, [=] __device__(int64_t i) {
     const int64_t b = elem_of(g, i);
     if (!onfine[b]) return;
-    sel[i] = (!is_pad(g, i - b * g.field) && t1[i] < T(0.5) && omc[i] < inf_t<T>()) ? 1 : 0;
+    sel[i] = (!is_pad_b(g, b, i - b * g.field) && t1[i] < T(0.5) && omc[i] < inf_t<T>()) ? 1 : 0;
   });
   Sel<T> ss{};
   ss.src = SelSrc::kField;
@@ -1086,7 +1086,8 @@ bool Engine<T>::ladder_and_weights(int32_t* n_rungs_max) {
     double d_min, d_max;
     std::memcpy(&d_min, &e.d_min_bits, sizeof d_min);
     std::memcpy(&d_max, &e.d_max_bits, sizeof d_max);
-    const std::vector<int32_t> ladder = rung_ladder(d_min, d_max, e.w, c_.n_max);
+    const int32_t n_max = g_.len_host ? g_.len_host[b] : c_.n_max;
+    const std::vector<int32_t> ladder = rung_ladder(d_min, d_max, e.w, n_max);
     if (ladder.empty() || static_cast<int32_t>(ladder.size()) > kMaxRungs) throw std::logic_error("eda: ladder size out of range");
     e.n_rungs = static_cast<int32_t>(ladder.size());
     for (int32_t j = 0; j < kMaxRungs; ++j) e.rung_w[j] = j < e.n_rungs ? ladder[static_cast<size_t>(j)] : 0;
@@ -1395,7 +1396,7 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
     const int64_t v = i - b * g.field;
     const int64_t q = pitch_row(g, v);
     const int64_t t = v - q * g.pitch;
-    r[i] = t < nl ? x[b * g.count + q * nl + t] : T(0);
+    r[i] = t < (g.len ? elem_len(g, b) : nl) ? x[b * g.count + q * nl + t] : T(0);
   });
   EDAB_CUDA(cudaMemsetAsync(nonfin_, 0, sizeof(uint64_t) * B_, s_));
   EDAB_CUDA(cudaMemsetAsync(el_, 0, sizeof(Elem) * B_, s_));
@@ -1490,13 +1491,13 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
       for_elements(s_, B_, [=] __device__(int64_t b) {
         Elem& e = el[b];
         if (e.status != kActive) return;
-        const uint64_t N = static_cast<uint64_t>(g.count);
+        const uint64_t N = static_cast<uint64_t>(elem_count(g, b));
         uint64_t S2 = 0;
         bool enough = false;
         for (int a = 0; a < g.dim; ++a) {
           const uint64_t ea = e.ext[a];
           S2 += ea * ea;
-          if (ea * static_cast<uint64_t>(g.n[a]) >= 3 * N) enough = true;
+          if (ea * static_cast<uint64_t>(elem_n(g, b, a)) >= 3 * N) enough = true;
         }
         for (int a = 0; a < kMaxDim; ++a) e.ext[a] = 0;
         if (!enough) {
@@ -1512,7 +1513,7 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
         int32_t w = 2 * static_cast<int32_t>(floor((v > 1.0 ? v : 1.0) / 2.0)) + 1;
         w = max(w, 3);
         w = max(w, e.w_prev + 2);
-        if (w > c.n_max) {
+        if (w > (g.len ? elem_len(g, b) : c.n_max)) {
           leave(e, winp, maskp, B, b, kDone);
           return;
         }
@@ -1548,7 +1549,7 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
       }
       if (c.growth > 1.0 && e.k >= c.growth_from) {
         w = max(w, odd_window(__dmul_rn(c.growth, static_cast<double>(e.w_prev))));
-        if (w > c.n_max) {
+        if (w > (g.len ? elem_len(g, b) : c.n_max)) {
           leave(e, winp, maskp, B, b, kDone);
           return;
         }
@@ -1608,7 +1609,9 @@ void Engine<T>::run(const T* x, T* rows_out, int32_t* hist_scale, int32_t* hist_
       const int64_t b = idx / per;
       const int32_t k = el[b].exp;
       if (k == 0 || el[b].status == kError) return;
-      if ((idx - b * per) / g.count > el[b].n_imfs) return;
+      const int64_t at = idx - b * per;
+      if (at / g.count > el[b].n_imfs) return;
+      if (g.len && at % g.count >= elem_len(g, b)) return;  // beyond the element's length: never written
       const T v = times_pow2(rows[idx], k);
       rows[idx] = v;
       if (!isfinite(v)) el[b].error = kErrNonFiniteResult;

@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(256) riesz_spectrum(Geom g, int kind, int a, i
     for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < g.field;
          v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       int32_t k[kMaxDim];
-      if (!voxel_coords_d<D>(g, v, k)) continue;
+      if (!voxel_coords_d<D>(g, v, g.n[D - 1], k)) continue;
       const int64_t i = e * g.field + v;
       Y[i] = static_cast<T>(__dmul_rn(riesz_mult<D>(g, kind, a, b, k), static_cast<double>(X[i])));
     }

@@ -39,10 +39,10 @@ __global__ void __launch_bounds__(kThreads) row_partials(const T* __restrict__ f
                                                          uint64_t* nonfinite) {
   const int lane = threadIdx.x & 31;
   const int64_t total = g.batch * g.rows;
-  const int32_t n = g.n_last;
-  const int32_t nchunks = (n + 31) >> 5;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
   for (int64_t q = blockIdx.x * static_cast<int64_t>(kThreads / 32) + (threadIdx.x >> 5); q < total; q += warps) {
+    const int32_t n = g.len ? elem_len(g, q / g.rows) : g.n_last;
+    const int32_t nchunks = (n + 31) >> 5;
     const T* row = f + q * g.pitch;
     uint64_t amax = 0;
     unsigned bad = 0;
@@ -205,7 +205,7 @@ struct SelView {
 template <class T>
 __device__ __forceinline__ bool sel_raw(const Geom& g, const SelView<T>& a, int64_t b, int64_t t, T* out) {
   if (a.sel.src == SelSrc::kField) {
-    if (is_pad(g, t)) return false;
+    if (is_pad_b(g, b, t)) return false;
     const int64_t i = b * g.field + t;
     if (a.sel.mask != nullptr && (a.sel.mask[i] & a.sel.bits) == 0) return false;
     *out = a.sel.field[i];
@@ -214,7 +214,7 @@ __device__ __forceinline__ bool sel_raw(const Geom& g, const SelView<T>& a, int6
   const int64_t k = static_cast<int64_t>(__umul64hi(static_cast<uint64_t>(t), g.field_inv));  // t < 3 field
   const int64_t v = t - k * g.field;
   const int axis = k == 0 ? a.ax[0] : (k == 1 ? a.ax[1] : a.ax[2]);
-  if (is_pad(g, v) || coord_of(g, v, axis) >= geom_n(g, axis) - 1) return false;
+  if (is_pad_b(g, b, v) || coord_of(g, v, axis) >= elem_n(g, b, axis) - 1) return false;
   const int64_t i = b * g.field + v;
   const int64_t st = axis == g.dim - 1 ? 1 : geom_stride(g, axis);
   *out = sub_rn(a.sel.field[i + st], a.sel.field[i]);
@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(kThreads) flags_pass(Geom g, int axis, const T
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
-  const int32_t n = geom_n(g, axis);
+  const int32_t n = elem_n(g, b, axis);
   const bool contig = axis == g.dim - 1;
   const int32_t nb = (n + kBlk - 1) / kBlk;
   T* X = reinterpret_cast<T*>(smem_raw);
@@ -890,7 +890,7 @@ __global__ void __launch_bounds__(kThreads) flags_long(Geom g, const T* __restri
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
   const int64_t row = blockIdx.x;
-  const int32_t n = g.n_last;
+  const int32_t n = elem_len(g, b);
   const int32_t nb = (n + kBlk - 1) / kBlk;
   T* bmin = reinterpret_cast<T*>(smem_raw);
   T* bmax = bmin + nb;
@@ -999,7 +999,7 @@ __global__ void __launch_bounds__(kThreads) ccl_tiles(Geom g, const uint8_t* __r
   __shared__ int32_t P[kTileWords];
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
-  const int32_t pitch = static_cast<int32_t>(g.pitch), nl = g.n_last;
+  const int32_t pitch = static_cast<int32_t>(g.pitch), nl = elem_len(g, b);
   const int32_t col_tiles = (pitch + tile_cols - 1) / tile_cols;
   const int64_t row0 = static_cast<int64_t>(blockIdx.x / col_tiles) * tile_rows;
   const int32_t c0 = static_cast<int32_t>(blockIdx.x % col_tiles) * tile_cols;
@@ -1107,7 +1107,7 @@ void ccl(cudaStream_t s, const Geom& g, const uint8_t* mask, uint8_t bits, int32
                if (L[v] < 0) return;
                const int64_t row = pitch_row(g, v);
                const int64_t col = v - row * g.pitch;
-               if (wide && (col + 1) % tile_cols == 0 && col + 1 < g.n_last && L[v + 1] >= 0) {
+               if (wide && (col + 1) % tile_cols == 0 && col + 1 < elem_len(g, b) && L[v + 1] >= 0) {
                  uf_join<true>(L, static_cast<int32_t>(v), static_cast<int32_t>(v + 1));
                }
                const int64_t tile = row / tile_rows;

@@ -34,6 +34,8 @@ __all__ = [
     "autotune",
     "load_tuning",
     "monogenic",
+    "length_classes",
+    "set_length_classes",
     "set_transform_precision",
     "transform_precision",
 ]
@@ -56,6 +58,20 @@ def set_transform_precision(name: str) -> None:
 def transform_precision() -> str:
     """The current product of the float32 orientation transforms (see set_transform_precision)."""
     return TRANSFORM_PRECISIONS[_native.core().transform_precision()]
+
+
+def set_length_classes(on: bool) -> None:
+    """How decompose_ragged groups 1-D signals, for the whole process: True (the default) decomposes
+    the signals whose lengths share a class [2^k, 2^(k+1)) together as one batch of uneven lengths,
+    False groups them by exact length. Results are the same either way (every signal's rows and
+    information are those of a call on that signal alone). This engine's extension: the reference
+    takes one shape per call."""
+    _native.core().set_length_classes(bool(on))
+
+
+def length_classes() -> bool:
+    """Whether decompose_ragged groups 1-D signals by length class (see set_length_classes)."""
+    return _native.core().length_classes()
 
 
 def build_info() -> dict[str, Any]:

@@ -417,8 +417,9 @@ def decompose_ragged(
     one device). Returns the list of each field's rows ``(P_i, *x_i.shape)`` (P_i = its IMF count
     plus the residue; a failed field's row is NaN), and with ``return_info`` the list of its
     ``DecompositionInfo`` (batch shape ``()``). Every field's result is the one ``eda.decompose``
-    gives for it alone; the fields are grouped by shape and up to ``workers`` groups run
-    concurrently on the GPU. The argument and error rules are those of ``eda.decompose``
+    gives for it alone; the fields are grouped (2-D and 3-D fields by shape; 1-D signals by length
+    class [2^k, 2^(k+1)), each class one batch of uneven lengths, see ``eda.set_length_classes``)
+    and up to ``workers`` groups run concurrently on the GPU. The argument and error rules are those of ``eda.decompose``
     (``errors='raise'`` raises DecompositionError naming the failed indices)."""
     max_imf = max(-_INT32_MAX - 1, min(_int_arg(max_imf, "max_imf"), _INT32_MAX))
     tie = _tie(tie_tolerance)

@@ -79,6 +79,8 @@ class Core:
         L.eda_ragged_free.restype = None
         L.eda_set_transform_precision.argtypes = [ctypes.c_int]
         L.eda_transform_precision.argtypes = []
+        L.eda_set_length_classes.argtypes = [i32]
+        L.eda_length_classes.argtypes = []
         L.eda_buffer_alloc.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(vp), ctypes.POINTER(vp)]
         L.eda_buffer_release.argtypes = [vp]
         L.eda_buffer_release.restype = None
@@ -146,6 +148,13 @@ class Core:
 
     def transform_precision(self) -> int:
         return int(self._lib.eda_transform_precision())
+
+    # -- how ragged 1-D batches group their signals -------------------------------------------
+    def set_length_classes(self, on: bool) -> None:
+        self._check(self._lib.eda_set_length_classes(1 if on else 0))
+
+    def length_classes(self) -> bool:
+        return bool(self._lib.eda_length_classes())
 
     # -- errors --------------------------------------------------------------------------------
     def _check(self, status: int) -> None:

@@ -143,9 +143,10 @@ EDA_API int eda_monogenic(const void* x, int x_on_device, int dtype, int dim, in
 /* Ragged batches: count elements of different shapes (same dtype and dim) in one call. Element i is
  * the C-contiguous array x[i] with extents n[i * dim .. i * dim + dim - 1], all on the host
  * (x_on_device 0) or all on the calling thread's current device and ready once `stream` (a
- * cudaStream_t; NULL: the legacy default stream) reaches the call. Equal shapes are decomposed
- * together and up to `workers` groups run concurrently, each on its own stream and workspace; every
- * element's rows and information are those a one-element eda_decompose call gives. The reference
+ * cudaStream_t; NULL: the legacy default stream) reaches the call. Equal shapes (1-D signals: length
+ * classes, eda_set_length_classes) are decomposed together and up to `workers` groups run
+ * concurrently, each on its own stream and workspace; every element's rows and information are
+ * those a one-element eda_decompose call gives. The reference
  * takes one shape per call (cpp/src/decompose.hpp:106): a ragged workload there is one call per
  * shape. On EDA_OK *out receives the run, released by eda_ragged_free. */
 typedef struct eda_ragged_run eda_ragged_run;
@@ -216,6 +217,15 @@ EDA_API int eda_tuning_clear(void);
  * the field for 3xTF32 and FP32, 1e-5 for BF16x3). eda_transform_precision returns the current one. */
 EDA_API int eda_set_transform_precision(int mode);
 EDA_API int eda_transform_precision(void);
+
+/* How eda_decompose_ragged groups 1-D signals, process-wide (no counterpart in the reference, which
+ * takes one shape per call, cpp/src/decompose.hpp:106): non-zero (the default) = by length class,
+ * the lengths in [2^k, 2^(k+1)) decomposed together as one batch of uneven lengths (every kernel
+ * reads each signal's own length); 0 = by exact length. Either way every signal's rows and
+ * information are those of a one-element eda_decompose call. eda_length_classes returns the
+ * current setting (1 or 0). */
+EDA_API int eda_set_length_classes(int32_t on);
+EDA_API int eda_length_classes(void);
 
 /* The allocation-free decomposition (no counterpart in the reference), for callers that must not
  * allocate device memory: plugin hosts whose device allocator belongs to the host application, and

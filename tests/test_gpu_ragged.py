@@ -148,3 +148,88 @@ def test_fresh_workspaces_are_zeroed_on_the_workers_streams(torch):
             assert same(np.asarray(rows[i]), np.asarray(want)), i
             assert int(infos[i].n_imfs) == int(winfo.n_imfs[0])
     torch.cuda.synchronize()
+
+
+@pytest.fixture
+def exact_lengths():
+    """Runs a test body with 1-D signals grouped by exact length, restoring length classes after."""
+    import eda
+
+    eda.set_length_classes(False)
+    try:
+        yield
+    finally:
+        eda.set_length_classes(True)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_length_classes_equal_exact_length_groups(torch, dtype):
+    """Signals of one length class run as one batch of uneven lengths (every kernel reading each
+    signal's own length); grouped by exact length every signal runs alone. Both must agree bit for
+    bit, and with one call per signal."""
+    import eda
+
+    assert eda.length_classes()
+    lengths = [2, 3, 31, 32, 33, 63, 64, 65, 100, 127, 250, 256, 300, 511, 640, 1000, 1023]
+    xs = [signal(n, 500 + i).astype(dtype) for i, n in enumerate(lengths)]
+    rows_c, infos_c = eda.decompose_ragged(xs, return_info=True)
+    eda.set_length_classes(False)
+    try:
+        rows_e, infos_e = eda.decompose_ragged(xs, return_info=True)
+    finally:
+        eda.set_length_classes(True)
+    for i in range(len(xs)):
+        assert same(np.asarray(rows_c[i]), np.asarray(rows_e[i])), lengths[i]
+        assert int(infos_c[i].n_imfs) == int(infos_e[i].n_imfs)
+        np.testing.assert_array_equal(infos_c[i].windows, infos_e[i].windows)
+        np.testing.assert_array_equal(infos_c[i].energy, infos_e[i].energy)
+    check_against_alone(eda, xs[::4], rows_c[::4], infos_c[::4])
+
+
+def test_length_class_across_the_staged_capacity(torch):
+    """A class whose longest signal folds its lines in global memory (beyond the shared-memory
+    capacity of a staged cube pass) runs every signal of the class that way, signals that alone
+    would be staged included: the canonical folds make both give the same bits."""
+    import eda
+
+    lengths = [16400, 20000, 16384, 18000, 30000]
+    xs = [signal(n, 900 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    rows, infos = eda.decompose_ragged(xs, return_info=True)
+    check_against_alone(eda, xs, rows, infos)
+
+
+def test_length_class_of_the_longest_signals(torch):
+    """The class [32768, 65536]: global-memory folds, the global-memory extrema pass (lines beyond
+    the staged extrema capacity) and column tiles in the components."""
+    import eda
+
+    lengths = [65536, 40000, 52000, 33000]
+    xs = [signal(n, 1300 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    rows, infos = eda.decompose_ragged(xs, return_info=True, workers=2)
+    check_against_alone(eda, xs, rows, infos)
+
+
+def test_length_class_device_input_and_failed_signal(torch):
+    import eda
+
+    lengths = [600, 900, 1000, 513, 700]
+    xs = [signal(n, 70 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    xs[2][400] = np.inf
+    xd = [torch.from_numpy(x).cuda() for x in xs]
+    rows, infos = eda.decompose_ragged(xd, return_info=True, errors="status")
+    assert int(infos[2].error) == 1 and rows[2].shape == (1, 1000)
+    host, hinfos = eda.decompose_ragged(xs, return_info=True, errors="status")
+    for i in range(len(xs)):
+        r = rows[i].cpu().numpy() if hasattr(rows[i], "cpu") else np.asarray(rows[i])
+        assert same(r, np.asarray(host[i])), i
+    keep = [0, 1, 3, 4]
+    check_against_alone(eda, [xs[i] for i in keep], [host[i] for i in keep], [hinfos[i] for i in keep])
+
+
+def test_exact_length_groups_still_equal_one_call_per_field(torch, exact_lengths):
+    import eda
+
+    lengths = [300, 511, 300, 777, 513]
+    xs = [signal(n, 31 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    rows, infos = eda.decompose_ragged(xs, return_info=True)
+    check_against_alone(eda, xs, rows, infos)
