@@ -455,6 +455,7 @@ def run_other(args) -> None:
     desc, data, axes, elements = other_workload(args.workload, 2024)
     ragged = axes is None
     if ragged:
+        eda.set_length_classes(not args.exact_lengths)
         on_dev = [torch.from_numpy(x).to(dev) for x in data]
         call_dev = lambda: eda.decompose_ragged(on_dev, workers=args.workers)  # noqa: E731
         call_host = lambda: eda.decompose_ragged(data, workers=args.workers)  # noqa: E731
@@ -535,7 +536,9 @@ def run_other(args) -> None:
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": desc, "l2": "flushed between steps (256 MiB write)",
-                   **({"workers": args.workers} if ragged else {})},
+                   **({"workers": args.workers,
+                       "grouping": "exact shapes" if args.exact_lengths or data[0].ndim > 1 else "1-D length classes"}
+                      if ragged else {})},
         "e2e": {"value": elements * args.steps / (sum(wall) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
@@ -580,6 +583,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling runs)")
     ap.add_argument("--workers", type=int, default=8,
                     help="concurrent shape groups of the ragged workloads (host threads with their own streams)")
+    ap.add_argument("--exact-lengths", action="store_true",
+                    help="ragged 1-D workloads: group the signals by exact length instead of length class")
     ap.add_argument("--tune", action="store_true",
                     help="autotune the cube passes' launch shapes for the workload's geometry before the warm-up "
                          "(on the 2-D workload the tuner keeps the default shape)")
