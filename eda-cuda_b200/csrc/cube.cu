@@ -1059,10 +1059,10 @@ void launch_long(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   long_line_input<T><<<blocks_for(g.batch * g.pitch), kThreads, 0, s>>>(g, a, keys);
   EDAB_LAUNCH("long_line_input");
   const size_t smem = static_cast<size_t>(2) * tot_slots(g.n_last) * sizeof(T);
-  if (first_on_device(reinterpret_cast<const void*>(cube_long<T>))) {
+  once_on_device(reinterpret_cast<const void*>(cube_long<T>), [] {
     EDAB_CUDA(cudaFuncSetAttribute(cube_long<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(dev_facts().smem)));
-  }
+  });
   if (smem > dev_facts().smem) throw std::invalid_argument("edab: a line is too long for the long-line cube pass");
   if (g.batch > 0x7fffffffLL || a.rungs > 65535) throw std::invalid_argument("edab: cube launch too large");
   a.bytes = cube_bytes_counter();

@@ -13,6 +13,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -44,9 +45,11 @@ void cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 // Every kernel launch of the engine is followed by EDAB_LAUNCH: it checks the launch and counts it
 // for the instrumentation (profile.cu).
 void note_launch();
-// True on the first call for `key` (a kernel) on the current device, false after: kernel
-// attributes such as the dynamic shared-memory limit are set per device. Thread-safe.
-bool first_on_device(const void* key);
+// Runs set(), which sets attributes of kernel `key` on the current device (such as its dynamic
+// shared-memory limit: they are per device), on the first call for that kernel and device. Every
+// other call, from any host thread, returns only once set() has completed, so no launch can
+// overtake the attributes it needs; a set() that throws leaves the kernel to the next call.
+void once_on_device(const void* key, const std::function<void()>& set);
 #define EDAB_LAUNCH(name)            \
   do {                               \
     ::edab::note_launch();           \

@@ -414,9 +414,9 @@ CUtensorMap make_map(const void* base, bool bf16, uint64_t inner, uint64_t outer
 
 template <bool BF16>
 void set_smem_once() {
-  if (first_on_device(reinterpret_cast<const void*>(gemm_tc<BF16>))) {
+  once_on_device(reinterpret_cast<const void*>(gemm_tc<BF16>), [] {
     EDAB_CUDA(cudaFuncSetAttribute(gemm_tc<BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, Stage<BF16>::kSmem));
-  }
+  });
 }
 
 }  // namespace tc

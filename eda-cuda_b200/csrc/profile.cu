@@ -27,13 +27,15 @@ __device__ unsigned long long g_cube_bytes;
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-bool first_on_device(const void* key) {
+void once_on_device(const void* key, const std::function<void()>& set) {
   static std::mutex mu;
   static std::set<std::pair<int, const void*>> seen;
   int dev = 0;
   EDAB_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(mu);
-  return seen.emplace(dev, key).second;
+  std::lock_guard<std::mutex> lock(mu);  // held while set() runs: later callers wait for it
+  if (seen.count({dev, key})) return;
+  set();
+  seen.emplace(dev, key);
 }
 
 bool profiling() { return g_on.load(std::memory_order_relaxed); }

@@ -173,6 +173,11 @@ namespace cg = cooperative_groups;
 constexpr int kDigitBits = 11;
 constexpr int kDigitBins = 1 << kDigitBits;
 constexpr int kSelClusterMax = 8;
+// The cluster form for batches that fill the GPU with clusters (1), or the grid-wide form always (0).
+#ifndef EDAB_SEL_CLUSTERS
+#define EDAB_SEL_CLUSTERS 1
+#endif
+constexpr bool kSelClusters = EDAB_SEL_CLUSTERS != 0;
 constexpr size_t kSelSmem = 2 * kDigitBins * sizeof(unsigned long long) + 2 * kDigitBins * sizeof(uint32_t);
 
 __device__ __forceinline__ uint32_t order_key(float v) {
@@ -590,14 +595,18 @@ size_t select_scratch_bytes(const Geom& g) {
 // [B][2][bins] count tables, zeroed here and left zeroed by every pick).
 template <class T, class K>
 void select_grid(cudaStream_t s, const Geom& g, const SelView<T>& a, double q, const int32_t* run, double* out,
-                 int64_t* count, void* scratch) {
+                 int64_t* count, void* scratch, int sms) {
   constexpr int kDigits = (8 * static_cast<int>(sizeof(K)) + kDigitBits - 1) / kDigitBits;
   auto* st = static_cast<SelGridState<K>*>(scratch);
   auto* table = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) +
                                                        align256(static_cast<size_t>(g.batch) * sizeof(SelGridState<uint64_t>)));
   EDAB_CUDA(cudaMemsetAsync(table, 0, static_cast<size_t>(g.batch) * 2 * kDigitBins * sizeof(unsigned long long), s));
-  const int64_t per_cta = int64_t{kThreads} * 64;
-  const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>((a.items + per_cta - 1) / per_cta, 1, 1024));
+  // CTAs per element: 64 items per thread, and for small batches enough CTAs for 8 per SM (at
+  // least 4 items per thread)
+  const int64_t by_items = (a.items + int64_t{kThreads} * 64 - 1) / (int64_t{kThreads} * 64);
+  const int64_t fill = std::min<int64_t>((int64_t{8} * sms + g.batch - 1) / g.batch,
+                                         std::max<int64_t>(1, a.items / (int64_t{kThreads} * 4)));
+  const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>(std::max(by_items, fill), 1, 1024));
   for (int pass = 0; pass < kDigits; ++pass) {
     select_grid_count<T, K><<<dim3(ctas, static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(g, a, run, st, table, pass);
     EDAB_LAUNCH("select_grid_count");
@@ -628,15 +637,15 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
     EDAB_CUDA(cudaGetDevice(&dev));
     EDAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   }
-  if (g.batch * kSelClusterMax < 2 * static_cast<int64_t>(sms)) {
+  if (!kSelClusters || g.batch * kSelClusterMax < 2 * static_cast<int64_t>(sms)) {
     if (!scratch) throw std::logic_error("edab: the grid-wide selection needs its scratch");
     if constexpr (std::is_same_v<T, float>) {
       if (sel.center == nullptr) {
-        select_grid<T, uint32_t>(s, g, a, q, run, out, count, scratch);
+        select_grid<T, uint32_t>(s, g, a, q, run, out, count, scratch, sms);
         return;
       }
     }
-    select_grid<T, uint64_t>(s, g, a, q, run, out, count, scratch);
+    select_grid<T, uint64_t>(s, g, a, q, run, out, count, scratch, sms);
     return;
   }
   // CTAs per element: about 16 items per thread, up to a cluster of 8
@@ -655,9 +664,9 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   const auto launch = [&](auto kernel) {
-    if (first_on_device(reinterpret_cast<const void*>(kernel))) {
+    once_on_device(reinterpret_cast<const void*>(kernel), [&] {
       EDAB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSelSmem)));
-    }
+    });
     EDAB_CUDA(cudaLaunchKernelEx(&cfg, kernel, g, a, run, q, out, count));
     EDAB_LAUNCH("select_cluster");
   };
@@ -1051,9 +1060,9 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
   EDAB_CUDA(cudaGetDevice(&dev));
   EDAB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const size_t cap = static_cast<size_t>(optin) - 2048;
-  if (first_on_device(reinterpret_cast<const void*>(flags_pass<T>))) {  // the limit is per device
+  once_on_device(reinterpret_cast<const void*>(flags_pass<T>), [&] {  // the limit is per device
     EDAB_CUDA(cudaFuncSetAttribute(flags_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cap)));
-  }
+  });
   for (int a = 0; a < g.dim; ++a) {
     const int32_t n = g.n[a];
     if (n < 3) continue;
@@ -1068,9 +1077,9 @@ void sig_flags(cudaStream_t s, const Geom& g, const T* r, const T* tau, uint8_t*
       // a 1-D line beyond the staged capacity: samples from global memory, block extremes staged
       const size_t ext_bytes = static_cast<size_t>(2) * nb * sizeof(T);
       if (g.dim != 1 || ext_bytes > cap) throw std::invalid_argument("edab: a line exceeds the shared memory of the extrema pass");
-      if (first_on_device(reinterpret_cast<const void*>(flags_long<T>))) {
+      once_on_device(reinterpret_cast<const void*>(flags_long<T>), [&] {
         EDAB_CUDA(cudaFuncSetAttribute(flags_long<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cap)));
-      }
+      });
       flags_long<T><<<dim3(static_cast<unsigned>(g.rows), static_cast<unsigned>(g.batch)), kThreads, ext_bytes, s>>>(
           g, r, tau, flags, el, run);
       EDAB_LAUNCH("flags_long");

@@ -233,3 +233,15 @@ def test_exact_length_groups_still_equal_one_call_per_field(torch, exact_lengths
     xs = [signal(n, 31 + i).astype(np.float32) for i, n in enumerate(lengths)]
     rows, infos = eda.decompose_ragged(xs, return_info=True)
     check_against_alone(eda, xs, rows, infos)
+
+
+def test_length_classes_in_cluster_selections(torch):
+    """Classes of many signals (the exact selections run as thread-block clusters, one per
+    signal, from several host threads at once) still equal one call per signal."""
+    import eda
+
+    rng = np.random.default_rng(77)
+    lengths = [int(v) for v in rng.integers(256, 1024, size=96)]
+    xs = [signal(n, 2000 + i).astype(np.float32) for i, n in enumerate(lengths)]
+    rows, infos = eda.decompose_ragged(xs, return_info=True, workers=8)
+    check_against_alone(eda, xs, rows, infos)
