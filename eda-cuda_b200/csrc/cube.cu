@@ -38,7 +38,16 @@ namespace edab {
 namespace {
 
 constexpr int kOpMaxK = 0, kOpMinK = 1, kOpSum = 2;
-constexpr int kWarps = kThreads / 32;
+// Threads of a cube CTA, and CTAs per SM the registers are bounded for (build-time choices; the
+// lines, groups and segment share of a launch are chosen at run time).
+#ifndef EDAB_CUBE_THREADS
+#define EDAB_CUBE_THREADS 256
+#endif
+#ifndef EDAB_CUBE_CTAS
+#define EDAB_CUBE_CTAS 4
+#endif
+constexpr int kCubeThreads = EDAB_CUBE_THREADS;
+constexpr int kWarps = kCubeThreads / 32;
 constexpr int kMaxGroupsPerCta = 4;  // line groups one CTA may run (the default launch shape runs one)
 // A window folds whole segments per worker when its segments number at least workers / seq_share
 // (the default, or the tuned value of the geometry).
@@ -651,10 +660,7 @@ struct Vec16<double> {
 };
 
 template <class T, int P, bool ROWS>
-#ifndef EDAB_CUBE_CTAS
-#define EDAB_CUBE_CTAS 4
-#endif
-__global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, PassArgs<T> a) {
+__global__ void __launch_bounds__(kCubeThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, PassArgs<T> a) {
   constexpr int VW = 16 / static_cast<int>(sizeof(T));  // samples per 16-byte copy
   constexpr int PP = ROWS ? 1 : P;                        // sample stride in shared memory
   using V16 = typename Vec16<T>::type;
@@ -682,7 +688,7 @@ __global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, Pa
   // the windows of this CTA's rungs, once
   if (threadIdx.x == 0) any_s = 0;
   __syncthreads();
-  for (int32_t jj = threadIdx.x; jj < nr; jj += kThreads) {
+  for (int32_t jj = threadIdx.x; jj < nr; jj += kCubeThreads) {
     const int32_t w = a.win[static_cast<int64_t>(j_begin + jj) * g.batch + b];
     Win q{};
     if (w >= 1) {
@@ -720,7 +726,7 @@ __global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, Pa
   const int32_t r_du = 32 * kWpl;
   const int c_q = threadIdx.x % QP;
   const int32_t c_i0 = threadIdx.x / QP;
-  const int32_t c_di = kThreads / QP;
+  const int32_t c_di = kCubeThreads / QP;
   const auto src_of = [&](int f) -> const T* {
     const T* s = (f == 0 || a.in1 == nullptr) ? a.in0 : a.in1;
     return s + static_cast<int64_t>(j_begin) * a.in_stride + eoff;
@@ -778,7 +784,7 @@ __global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, Pa
     } else {
       if (s.mask) {
         const int p = threadIdx.x % P;
-        for (int32_t i = threadIdx.x / P; i < n; i += kThreads / P) {
+        for (int32_t i = threadIdx.x / P; i < n; i += kCubeThreads / P) {
           const int64_t at = s.base + static_cast<int64_t>(i) * step + p;
           const T v = bits ? (((bits[at] >> a.bit) & 1u) ? T(1) : T(0)) : src[at];
           Vb[i * P + p] = box ? v : okey(v);
@@ -844,7 +850,7 @@ __global__ void __launch_bounds__(kThreads, EDAB_CUBE_CTAS) cube_pass(Geom g, Pa
       } else {
         const int p = threadIdx.x % P;
         if (!((s.mask >> p) & 1u)) return;
-        for (int32_t i = threadIdx.x / P; i < n; i += kThreads / P) {
+        for (int32_t i = threadIdx.x / P; i < n; i += kCubeThreads / P) {
           const int64_t at = s.base + static_cast<int64_t>(i) * step + p;
           dst[at] = epi(R[i * P + p], fac, detsq ? aux[at] : T(0));
         }
@@ -931,7 +937,7 @@ __global__ void __launch_bounds__(kThreads) long_line_input(Geom g, PassArgs<T> 
 }
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) cube_long(Geom g, PassArgs<T> a, const T* __restrict__ keys) {
+__global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a, const T* __restrict__ keys) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ Win q_s;
   __shared__ T fac_s;
@@ -1037,6 +1043,7 @@ int lines_per_cta(const Geom& g, int axis, size_t cap) {
   const bool rows = axis == g.dim - 1;
   int P = 8;
   if (rows) {
+    while (P > kWarps) P /= 2;  // rows: a warp (or more) stages and stores each line
     while (P > 1 && P / 2 >= g.rows) P /= 2;
   }
   while (P > 1 && smem_bytes(n, P, rows, sizeof(T)) > cap / 2) P /= 2;
@@ -1067,7 +1074,7 @@ void launch_long(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   if (g.batch > 0x7fffffffLL || a.rungs > 65535) throw std::invalid_argument("edab: cube launch too large");
   a.bytes = cube_bytes_counter();
   profile_cube_launch(s, true);
-  cube_long<T><<<dim3(static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs)), kThreads, smem, s>>>(g, a, keys);
+  cube_long<T><<<dim3(static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs)), kCubeThreads, smem, s>>>(g, a, keys);
   EDAB_LAUNCH("cube_long");
   profile_cube_launch(s, false);
 }
@@ -1084,7 +1091,7 @@ void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   }
   int P = lines_per_cta<T>(g, a.axis, f.smem);
   if (tune.lines > 0 && tune.lines <= 8 && smem_bytes(g.n[a.axis], tune.lines, rows, sizeof(T)) <= f.smem &&
-      (!rows || tune.lines <= std::max<int64_t>(1, g.rows))) {
+      (!rows || (tune.lines <= std::max<int64_t>(1, g.rows) && tune.lines <= kWarps))) {
     P = tune.lines;
   }
   if (a.rungs > kMaxRungs) throw std::invalid_argument("edab: more rungs than a cube launch holds");
@@ -1118,8 +1125,8 @@ void launch_pass(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   profile_cube_launch(s, true);
 #define EDAB_CUBE_LAUNCH(PV)                                                    \
   do {                                                                          \
-    if (rows) cube_pass<T, PV, true><<<grid, kThreads, smem, s>>>(g, a);        \
-    else cube_pass<T, PV, false><<<grid, kThreads, smem, s>>>(g, a);            \
+    if (rows) cube_pass<T, PV, true><<<grid, kCubeThreads, smem, s>>>(g, a);        \
+    else cube_pass<T, PV, false><<<grid, kCubeThreads, smem, s>>>(g, a);            \
   } while (0)
   switch (P) {
     case 1: EDAB_CUBE_LAUNCH(1); break;
