@@ -114,6 +114,10 @@ __device__ __forceinline__ T fold_identity() {
 
 struct Win {
   int32_t r, wa, o, k_lo, nseg, cps;
+  // the segments a CTA folds, relative to k_lo: segments [hk0, hk0 + hn) of the reversed line for
+  // H and [gk0, gk0 + gn) of the line for G (a whole line: 0 and nseg both; a tile of a long line:
+  // the segments its outputs need)
+  int32_t hk0, hn, gk0, gn;
 };
 // 32-bit arithmetic but for the offset's product (n (wa + 1) / 2 reaches 2^32 for the longest
 // lines; one 64-bit modulo per window set-up): the 64-bit integer divisions of a general formula
@@ -133,6 +137,8 @@ __device__ __forceinline__ Win make_win(int32_t n, int32_t w) {
   const int32_t k_hi = floor_div32(n - 1 + q.r - q.o, q.wa);
   q.nseg = k_hi - q.k_lo + 1;
   q.cps = (q.wa + 31) >> 5;
+  q.hk0 = q.gk0 = 0;
+  q.hn = q.gn = q.nseg;
   return q;
 }
 
@@ -435,11 +441,11 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   // phases. Windows of few, long segments (seq_share * nseg < workers) split their segments into
   // chunks over the workers instead: chunk totals, carries, then the H and G folds (four phases,
   // twice the folds, but every worker busy).
-  if (q.cps == 1 || q.nseg * seq_share >= workers) {
-    const int32_t per = (q.nseg + workers - 1) / workers;
-    const int32_t k_end = min((worker + 1) * per, q.nseg);
-    for (int32_t k = worker * per; k < k_end; ++k) {
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+  if (q.cps == 1 || max(q.hn, q.gn) * seq_share >= workers) {
+    const int32_t hper = (q.hn + workers - 1) / workers;
+    const int32_t hk_end = min((worker + 1) * hper, q.hn);
+    for (int32_t k = worker * hper; k < hk_end; ++k) {
+      const int32_t s = q.o + (q.k_lo + q.hk0 + k) * q.wa;
       const int32_t c1 = min(s + q.wa - 1, e_max);
       if (q.cps > 1) {
         seg_h<T, OP, PP>(Vp, Rp, n, q, s, c1);
@@ -452,8 +458,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
       }
     }
     __syncthreads();
-    for (int32_t k = worker * per; k < k_end; ++k) {
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t gper = (q.gn + workers - 1) / workers;
+    const int32_t gk_end = min((worker + 1) * gper, q.gn);
+    for (int32_t k = worker * gper; k < gk_end; ++k) {
+      const int32_t s = q.o + (q.k_lo + q.gk0 + k) * q.wa;
       const int32_t e_al = s + q.wa - 1;
       const int32_t c1 = min(e_al, e_max);
       if (q.cps > 1) {
@@ -482,8 +490,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     // phase 1: chunk totals; half of the workers take the line, half the reversed line
     constexpr int half = workers / 2;
     const int dir = worker >= half;
-    for (Tasks t(worker - dir * half, half, q.nseg); t.c < q.cps; t.next(q.nseg)) {
-      const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
+    const int32_t dn = dir ? q.hn : q.gn;
+    const int32_t dk0 = q.k_lo + (dir ? q.hk0 : q.gk0);
+    for (Tasks t(worker - dir * half, half, dn); t.c < q.cps; t.next(dn)) {
+      const int32_t s = q.o + (dk0 + t.k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t c0 = s + 32 * t.c;
       if (c0 > e_last) continue;
@@ -504,10 +514,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     }
     __syncthreads();
     // phase 2: exclusive carries per segment, in place (slot c holds the carry of chunk c >= 1)
-    for (int32_t t = worker; t < 2 * q.nseg; t += workers) {
-      const int dir = t >= q.nseg;
-      const int32_t k = t - dir * q.nseg;
-      const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    for (int32_t t = worker; t < q.gn + q.hn; t += workers) {
+      const int dir = t >= q.gn;
+      const int32_t k = t - dir * q.gn;
+      const int32_t s = q.o + (q.k_lo + (dir ? q.hk0 : q.gk0) + k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t nch = (e_last - s) / 32 + 1;
       T* tl = tot + (dir * TS + k * q.cps) * P + p;
@@ -521,8 +531,8 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     __syncthreads();
   }
   // phase 3: H (the reversed line's G) into R at the output slots n - 1 + r - e (e >= r)
-  for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
-    const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
+  for (Tasks t(worker, workers, q.hn); t.c < q.cps; t.next(q.hn)) {
+    const int32_t s = q.o + (q.k_lo + q.hk0 + t.k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
     const int32_t c0 = s + 32 * t.c;
     if (c0 > e_last) continue;
@@ -541,8 +551,8 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   }
   __syncthreads();
   // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r)), slot x = e - r
-  for (Tasks t(worker, workers, q.nseg); t.c < q.cps; t.next(q.nseg)) {
-    const int32_t s = q.o + (q.k_lo + t.k) * q.wa;
+  for (Tasks t(worker, workers, q.gn); t.c < q.cps; t.next(q.gn)) {
+    const int32_t s = q.o + (q.k_lo + q.gk0 + t.k) * q.wa;
     const int32_t e_al = s + q.wa - 1;
     const int32_t e_last = min(e_al, e_max);
     const int32_t c0 = s + 32 * t.c;
@@ -917,12 +927,16 @@ __global__ void __launch_bounds__(kCubeThreads, EDAB_CUBE_CTAS) cube_pass(Geom g
 
 // ---------------------------------------------------------------------------------------------
 // Lines too long to stage in shared memory (1-D signals beyond the staged capacity; the other
-// axes stay within it). The line's fold input (order keys for max / min, the samples or the
-// bit field's 0 / 1 for sums) is written once per element into a global scratch; then one CTA per
-// element and rung runs the same fold phases as the staged kernel with P = 1 on global memory (the
-// line and its outputs stay in L2), the chunk totals in shared memory, and the output line in the
-// rung's output field, finished in place by the pass's epilogue. The canonical folds, and so every
-// bit of the result, are those of the staged kernel.
+// axes stay within it). The line's fold input (order keys for max / min, the samples or the bit
+// field's 0 / 1 for sums) is written once per element into a global scratch (long_line_input).
+// Then the line is cut into tiles of kLongTile outputs, one CTA per tile, element and rung: the CTA
+// stages the samples of the segments its outputs need (x - r lies in a segment of the reversed
+// line, whose H it folds; x + r in a segment of the line, whose G it folds; every segment whole,
+// from its start, so every fold is the canonical one) and runs the staged kernel's fold phases on
+// them in shared memory. A window whose segments do not fit a tile's shared memory folds the whole
+// line in one CTA (the tile-0 CTA; the other tiles return) on global memory (the line and its
+// output stay in L2), with the chunk totals in shared memory. Every bit of the result is that of
+// the staged kernel.
 template <class T>
 __global__ void __launch_bounds__(kThreads) long_line_input(Geom g, PassArgs<T> a, T* keys) {
   const int64_t total = g.batch * g.pitch;  // 1-D: one row per element
@@ -936,56 +950,132 @@ __global__ void __launch_bounds__(kThreads) long_line_input(Geom g, PassArgs<T> 
   }
 }
 
+constexpr int32_t kLongTile = 4096;  // outputs per tile
+
+// The bounding interval [lo, hi] of the line samples that the extended positions [u, v] read
+// (reflect_index; -n <= u <= v < 2n).
+__device__ __forceinline__ void reflect_span(int32_t u, int32_t v, int32_t n, int32_t* lo, int32_t* hi) {
+  int32_t l = max(u, 0), h = min(v, n - 1);
+  if (u < 0) {
+    l = 0;
+    h = max(h, min(-u - 1, n - 1));
+  }
+  if (v > n - 1) {
+    h = n - 1;
+    l = min(l, max(2 * n - 1 - v, 0));
+  }
+  *lo = l;
+  *hi = h;
+}
+
 template <class T>
-__global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a, const T* __restrict__ keys) {
+__global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a, const T* __restrict__ keys,
+                                                         int32_t smem_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ Win q_s;
   __shared__ T fac_s;
-  const int64_t b = blockIdx.x;
-  const int32_t j = static_cast<int32_t>(blockIdx.y);
+  const int64_t b = blockIdx.y;
+  const int32_t j = static_cast<int32_t>(blockIdx.z);
   const int32_t n = elem_len(g, b);
+  const int32_t X0 = static_cast<int32_t>(blockIdx.x) * kLongTile;
+  if (X0 >= n) return;
   const int32_t w = a.win[static_cast<int64_t>(j) * g.batch + b];
   if (w < 1) return;
+  const int32_t X1 = min(X0 + kLongTile, n);
   const bool box = a.op == static_cast<int>(CubeOp::kBox);
-  if (threadIdx.x == 0) {
-    q_s = make_win(n, w);
-    if (box && a.last) fac_s = static_cast<T>(1.0 / static_cast<double>(2 * min((w - 1) / 2, n - 1) + 1));
-  }
-  __syncthreads();
-  const Win q = q_s;
-  const int32_t TS = tot_slots(n);
-  T* tot = reinterpret_cast<T*>(smem_raw);
-  const T* V = keys + b * g.pitch;
   const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
   const bool detsq = box && a.last && a.epi == static_cast<int>(BoxEpi::kDetSq);
-  for (int f = 0; f < nf; ++f) {
-    T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
-    const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-    if (box) run_stage<T, kOpSum, 1, 1>(V, R, tot, n, TS, q, 0, a.seq_share);
-    else if (is_min) run_stage<T, kOpMinK, 1, 1>(V, R, tot, n, TS, q, 0, a.seq_share);
-    else run_stage<T, kOpMaxK, 1, 1>(V, R, tot, n, TS, q, 0, a.seq_share);
-    // the epilogue in place (run_stage ended on a barrier: every output is written); pads are 0
-    const T* aux = detsq ? a.aux + b * g.field : nullptr;
-    for (int32_t i = threadIdx.x; i < static_cast<int32_t>(g.pitch); i += blockDim.x) {
-      T y = i < n ? R[i] : T(0);
-      if (i < n) {
-        if (!box) {
-          y = okey(y);
-        } else if (a.last) {
-          y = mul_rn(y, fac_s);
-          if (detsq) {
-            const T d = sub_rn(aux[i], y);
-            y = mul_rn(d, d);
+  const Win q = make_win(n, w);
+  if (threadIdx.x == 0 && box && a.last) fac_s = static_cast<T>(1.0 / static_cast<double>(q.wa));
+  // the tile's segments: G of the line's segments holding x + r, H of the reversed line's holding
+  // n - 1 - (x - r), for x in [X0, X1)
+  const int32_t e_max = n - 1 + q.r;
+  Win t = q;
+  t.gk0 = floor_div32(X0 + q.r - q.o, q.wa) - q.k_lo;
+  t.gn = floor_div32(X1 - 1 + q.r - q.o, q.wa) - q.k_lo - t.gk0 + 1;
+  t.hk0 = floor_div32(n - X1 + q.r - q.o, q.wa) - q.k_lo;
+  t.hn = floor_div32(n - 1 - X0 + q.r - q.o, q.wa) - q.k_lo - t.hk0 + 1;
+  const int32_t gs = q.o + (q.k_lo + t.gk0) * q.wa, ge = min(gs + t.gn * q.wa - 1, e_max);
+  const int32_t hs = q.o + (q.k_lo + t.hk0) * q.wa, he = min(hs + t.hn * q.wa - 1, e_max);
+  // the samples they read, and the output slots they write (H: n - 1 + r - e for e >= r; G: e - r)
+  int32_t glo, ghi, hlo, hhi;
+  reflect_span(gs, ge, n, &glo, &ghi);
+  reflect_span(hs, he, n, &hlo, &hhi);
+  const int32_t vlo = min(glo, n - 1 - hhi), vhi = max(ghi, n - 1 - hlo);
+  const int32_t xlo = min(max(gs, q.r) - q.r, n - 1 + q.r - he);
+  const int32_t xhi = max(ge - q.r, n - 1 + q.r - max(hs, q.r));
+  const int32_t nv = vhi - vlo + 1, nx = xhi - xlo + 1;
+  const int32_t TS = max(t.gn, t.hn) * q.cps;
+  const int32_t nv16 = (nv + 3) & ~3, nx16 = (nx + 3) & ~3;  // 16-byte aligned regions
+  const bool tiled = nv16 + nx16 + 2 * TS <= smem_elems;
+  if (!tiled && blockIdx.x != 0) return;  // the whole line folds in the tile-0 CTA
+  __syncthreads();
+  const T* line = keys + b * g.pitch;
+  unsigned long long acct = 0;
+  if (tiled) {
+    T* Vs = reinterpret_cast<T*>(smem_raw);
+    T* Rs = Vs + nv16;
+    T* tot = Rs + nx16;
+    for (int32_t i = threadIdx.x; i < nv; i += blockDim.x) Vs[i] = line[vlo + i];
+    __syncthreads();
+    for (int f = 0; f < nf; ++f) {
+      const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
+      // (the staged samples and slots at their line indices: only the staged ones are touched)
+      if (box) run_stage<T, kOpSum, 1, 1>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+      else if (is_min) run_stage<T, kOpMinK, 1, 1>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+      else run_stage<T, kOpMaxK, 1, 1>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+      T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
+      const T* aux = detsq ? a.aux + b * g.field : nullptr;
+      const int32_t end = X1 == n ? static_cast<int32_t>(g.pitch) : X1;  // the last tile writes the pads
+      for (int32_t x = X0 + threadIdx.x; x < end; x += blockDim.x) {
+        T y = T(0);
+        if (x < n) {
+          y = Rs[x - xlo];
+          if (!box) {
+            y = okey(y);
+          } else if (a.last) {
+            y = mul_rn(y, fac_s);
+            if (detsq) {
+              const T d = sub_rn(aux[x], y);
+              y = mul_rn(d, d);
+            }
           }
         }
+        R[x] = y;
       }
-      R[i] = y;
+      __syncthreads();  // the next field rewrites the slots and totals
     }
-    __syncthreads();
+    acct = static_cast<unsigned long long>(X1 - X0) * sizeof(T) * (1 + nf);
+  } else {
+    T* tot = reinterpret_cast<T*>(smem_raw);
+    const int32_t TSL = tot_slots(n);
+    for (int f = 0; f < nf; ++f) {
+      T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
+      const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
+      if (box) run_stage<T, kOpSum, 1, 1>(line, R, tot, n, TSL, q, 0, a.seq_share);
+      else if (is_min) run_stage<T, kOpMinK, 1, 1>(line, R, tot, n, TSL, q, 0, a.seq_share);
+      else run_stage<T, kOpMaxK, 1, 1>(line, R, tot, n, TSL, q, 0, a.seq_share);
+      // the epilogue in place (run_stage ended on a barrier: every output is written); pads are 0
+      const T* aux = detsq ? a.aux + b * g.field : nullptr;
+      for (int32_t i = threadIdx.x; i < static_cast<int32_t>(g.pitch); i += blockDim.x) {
+        T y = i < n ? R[i] : T(0);
+        if (i < n) {
+          if (!box) {
+            y = okey(y);
+          } else if (a.last) {
+            y = mul_rn(y, fac_s);
+            if (detsq) {
+              const T d = sub_rn(aux[i], y);
+              y = mul_rn(d, d);
+            }
+          }
+        }
+        R[i] = y;
+      }
+      __syncthreads();
+    }
+    acct = static_cast<unsigned long long>(n) * sizeof(T) * (1 + nf);
   }
-  if (a.bytes && threadIdx.x == 0) {
-    atomicAdd(a.bytes, static_cast<unsigned long long>(n) * sizeof(T) * (1 + nf));
-  }
+  if (a.bytes && threadIdx.x == 0) atomicAdd(a.bytes, acct);
 }
 
 thread_local void* t_long_scratch = nullptr;
@@ -1065,16 +1155,22 @@ void launch_long(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   T* keys = static_cast<T*>(t_long_scratch);
   long_line_input<T><<<blocks_for(g.batch * g.pitch), kThreads, 0, s>>>(g, a, keys);
   EDAB_LAUNCH("long_line_input");
-  const size_t smem = static_cast<size_t>(2) * tot_slots(g.n_last) * sizeof(T);
+  // shared memory: the whole-line fold's chunk totals, and at least half an SM's (two tile CTAs per
+  // SM) for the tiles' samples, slots and totals
+  const size_t whole = static_cast<size_t>(2) * tot_slots(g.n_last) * sizeof(T);
+  if (whole > dev_facts().smem) throw std::invalid_argument("edab: a line is too long for the long-line cube pass");
+  const size_t half_sm = (dev_facts().sm_smem / 2 - 2048) / 16 * 16;
+  const size_t smem = std::min(dev_facts().smem, std::max(whole, half_sm)) / 16 * 16;
   once_on_device(reinterpret_cast<const void*>(cube_long<T>), [] {
     EDAB_CUDA(cudaFuncSetAttribute(cube_long<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(dev_facts().smem)));
   });
-  if (smem > dev_facts().smem) throw std::invalid_argument("edab: a line is too long for the long-line cube pass");
-  if (g.batch > 0x7fffffffLL || a.rungs > 65535) throw std::invalid_argument("edab: cube launch too large");
+  const int64_t tiles = (g.n_last + kLongTile - 1) / kLongTile;
+  if (g.batch > 65535 || a.rungs > kMaxRungs) throw std::invalid_argument("edab: cube launch too large");
   a.bytes = cube_bytes_counter();
   profile_cube_launch(s, true);
-  cube_long<T><<<dim3(static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs)), kCubeThreads, smem, s>>>(g, a, keys);
+  const dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs));
+  cube_long<T><<<grid, kCubeThreads, smem, s>>>(g, a, keys, static_cast<int32_t>(smem / sizeof(T)));
   EDAB_LAUNCH("cube_long");
   profile_cube_launch(s, false);
 }

@@ -152,6 +152,15 @@ def test_cube_on_long_1d_lines(dev, n, op, dtype):
     check(dev, (n,), op, LONG_WINS[:4] if n == 8193 else LONG_WINS, dtype, seed=n)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", ["maxmin", "box"])
+def test_cube_long_line_tiles(dev, op, dtype):
+    """Long lines fold in tiles of 4096 outputs, each CTA staging the segments its outputs need,
+    or (windows whose segments do not fit a tile's shared memory) the whole line in one CTA: a
+    length that is no multiple of the tile, and windows on both sides of the limit."""
+    check(dev, (20001,), op, [5, 65, 1501, 2049, 2501, 3001, 4097, 6001, 9001], dtype, seed=21)
+
+
 def test_cube_rung_launch_on_long_lines(dev):
     rng = np.random.default_rng(5)
     wins = (2 * rng.integers(0, 3000, size=(4, 2)) + 1).astype(np.int32)
