@@ -168,6 +168,13 @@ int eda_ragged_collect(eda_ragged_run* run, int64_t i, void* dst, int dst_on_dev
   });
 }
 
+int eda_ragged_collect_all(eda_ragged_run* run, void* dst, int dst_on_device, const int64_t* offsets, void* stream) {
+  return guarded([&] {
+    if (!run) throw std::invalid_argument("eda: null run");
+    run->run->collect_all(dst, dst_on_device != 0, offsets, static_cast<cudaStream_t>(stream));
+  });
+}
+
 void eda_ragged_free(eda_ragged_run* run) { delete run; }
 
 int eda_run_shape(const eda_run* run, int64_t* batch, int32_t* rows, int32_t* K, int64_t* count, int64_t* chunk) {

@@ -288,6 +288,94 @@ void Run::collect_orientation(void* dir, void* coh, bool dst_on_device, cudaStre
   EDAB_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+
+// One element's rows of a ragged run's group, to be written at dst + dst_off.
+struct CollectItem {
+  int64_t src_off;   // (j cap) src_count: the element's first row in the group's rows
+  int64_t dst_off;
+  int64_t count;     // the element's samples per row
+  int32_t P, n_imfs, error;
+};
+
+// Blocks over the items (y) and over each item's P count samples (x).
+template <class T>
+__global__ void collect_items(const CollectItem* items, int64_t n_items, int64_t src_count, const T* __restrict__ src,
+                              T* __restrict__ dst) {
+  for (int64_t it = blockIdx.y; it < n_items; it += gridDim.y) {
+    const CollectItem c = items[it];
+    const int64_t total = static_cast<int64_t>(c.P) * c.count;
+    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const int64_t k = idx / c.count, t = idx - k * c.count;
+      T v;
+      if (c.error != 0) v = static_cast<T>(d_nan());
+      else if (k <= c.n_imfs) v = src[c.src_off + k * src_count + t];
+      else v = T(0);
+      dst[c.dst_off + idx] = v;
+    }
+  }
+}
+
+}  // namespace
+
+void RaggedRun::collect_all(void* dst, bool dst_on_device, const int64_t* offsets, cudaStream_t s) {
+  const int64_t count = static_cast<int64_t>(group.size());
+  if (count == 0) return;
+  if (!dst || !offsets) throw std::invalid_argument("eda: null argument");
+  const size_t es = dtype == 0 ? 4 : 8;
+  int prev = 0;
+  EDAB_CUDA(cudaGetDevice(&prev));
+  if (prev != device) EDAB_CUDA(cudaSetDevice(device));
+  // the extent of the destination, and every element's item in its group
+  int64_t total = 0;
+  std::vector<std::vector<CollectItem>> items(groups.size());
+  for (int64_t i = 0; i < count; ++i) {
+    const Run& r = *groups[static_cast<size_t>(group[static_cast<size_t>(i)])];
+    const int64_t j = index[static_cast<size_t>(i)];
+    CollectItem c{};
+    c.src_off = j * r.rows_cap * r.count;
+    c.dst_off = offsets[i];
+    c.count = r.count_of(j);
+    c.P = r.rows_of(j);
+    c.n_imfs = r.n_imfs[static_cast<size_t>(j)];
+    c.error = r.error[static_cast<size_t>(j)];
+    if (c.dst_off < 0) throw std::invalid_argument("eda: a negative destination offset");
+    total = std::max(total, c.dst_off + static_cast<int64_t>(c.P) * c.count);
+    items[static_cast<size_t>(group[static_cast<size_t>(i)])].push_back(c);
+  }
+  void* out = dst;
+  if (!dst_on_device) EDAB_CUDA(cudaMallocAsync(&out, static_cast<size_t>(total) * es, s));
+  std::vector<void*> tables;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    if (items[gi].empty()) continue;
+    const Run& r = *groups[gi];
+    void* tb = nullptr;
+    EDAB_CUDA(cudaMallocAsync(&tb, items[gi].size() * sizeof(CollectItem), s));
+    tables.push_back(tb);
+    EDAB_CUDA(cudaMemcpyAsync(tb, items[gi].data(), items[gi].size() * sizeof(CollectItem), cudaMemcpyHostToDevice, s));
+    const int64_t ni = static_cast<int64_t>(items[gi].size());
+    int64_t longest = 1;
+    for (const CollectItem& c : items[gi]) longest = std::max(longest, static_cast<int64_t>(c.P) * c.count);
+    const dim3 grid(std::min<unsigned>(blocks_for(longest), 256u), static_cast<unsigned>(std::min<int64_t>(ni, 65535)));
+    if (dtype == 0) {
+      collect_items<float><<<grid, kThreads, 0, s>>>(static_cast<const CollectItem*>(tb), ni, r.count,
+                                                     static_cast<const float*>(r.dev_rows), static_cast<float*>(out));
+    } else {
+      collect_items<double><<<grid, kThreads, 0, s>>>(static_cast<const CollectItem*>(tb), ni, r.count,
+                                                      static_cast<const double*>(r.dev_rows), static_cast<double*>(out));
+    }
+    EDAB_LAUNCH("collect_items");
+  }
+  if (!dst_on_device) {
+    copy_to_pageable(dst, out, static_cast<size_t>(total) * es, s);
+    EDAB_CUDA(cudaFreeAsync(out, s));
+  }
+  for (void* tb : tables) EDAB_CUDA(cudaFreeAsync(tb, s));
+  EDAB_CUDA(cudaStreamSynchronize(s));
+  if (prev != device) EDAB_CUDA(cudaSetDevice(prev));
+}
+
 void Run::collect_one(int64_t j, void* dst, bool dst_on_device, cudaStream_t s) {
   if (j < 0 || j >= batch) throw std::invalid_argument("eda: element index out of range");
   const size_t es = dtype == 0 ? 4 : 8;

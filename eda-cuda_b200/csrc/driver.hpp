@@ -114,6 +114,10 @@ struct RaggedRun {
   std::vector<std::unique_ptr<Run>> groups;
   std::vector<int32_t> group;   // per element: its group
   std::vector<int64_t> index;   // per element: its index in the group
+  // Every element's rows (P_i, count_i) into one buffer dst (host, or device memory of the run's
+  // device) at dst + offsets[i] samples: one table copy and one kernel per group (and, for a host
+  // dst, one device-to-host copy of all of them). Complete on return.
+  void collect_all(void* dst, bool dst_on_device, const int64_t* offsets, cudaStream_t s);
 };
 // xs[i]: element i, C-contiguous with extents n[i * dim .. i * dim + dim - 1]; on_device: every
 // element on the current device, ready once `s` reaches the call. workers: concurrent groups (>= 1).

@@ -479,22 +479,22 @@ def decompose_ragged(
         with torch.cuda.device(device):
             st = torch.cuda.current_stream(device)
 
-            def out_of(P, shape):
-                out = torch.empty((P,) + shape, dtype=tdt, device=device)
+            def alloc(total):
+                out = torch.empty((max(total, 1),), dtype=tdt, device=device)
                 return out, out.data_ptr()
 
             res = core.decompose_ragged([t.data_ptr() for t in ts], True, target, shapes, max_imf, tie, sifts,
-                                        check_finite, workers, st.cuda_stream, out_of)
+                                        check_finite, workers, st.cuda_stream, alloc)
         rows = [_device.DeviceArray(r) for r, _ in res]
     else:
         hs = [np.ascontiguousarray(f if f.dtype == np.dtype(target) else f.astype(target)) for f in fields]
 
-        def out_of(P, shape):
-            out = np.empty((P,) + shape, target)
+        def alloc(total):
+            out = np.empty((max(total, 1),), target)
             return out, out.ctypes.data
 
         res = core.decompose_ragged([h.ctypes.data for h in hs], False, target, shapes, max_imf, tie, sifts,
-                                    check_finite, workers, 0, out_of)
+                                    check_finite, workers, 0, alloc)
         rows = [r for r, _ in res]
     infos = []
     for (_, raw), shape in zip(res, shapes):

@@ -73,6 +73,7 @@ class Core:
                                            ctypes.POINTER(i64), ctypes.POINTER(_Params), i32, vp, ctypes.POINTER(vp)]
         L.eda_ragged_element.argtypes = [vp, i64] + [vp] * 7
         L.eda_ragged_collect.argtypes = [vp, i64, vp, ctypes.c_int, vp]
+        L.eda_ragged_collect_all.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(i64), vp]
         L.eda_monogenic.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, i64, ctypes.POINTER(i64), i64, vp,
                                     ctypes.c_int, ctypes.POINTER(i32), vp]
         L.eda_ragged_free.argtypes = [vp]
@@ -304,12 +305,13 @@ class Core:
 
     def decompose_ragged(self, ptrs: list[int], on_device: bool, dtype: str, shapes: list[tuple[int, ...]],
                          max_imf: int, tie_tolerance: float | None, sifts: int, check_finite: bool, workers: int,
-                         stream: int, out_of) -> list[tuple[Any, dict]]:
+                         stream: int, alloc) -> list[tuple[Any, dict]]:
         """Decomposes len(ptrs) C-contiguous arrays of one dtype and one number of axes, each of its own
         shape, on the host or on the current device (ready once ``stream`` reaches the call);
-        ``out_of(P, shape)`` allocates an element's (P, *shape) output and returns it with its
-        pointer. Returns (rows, info) per element; info holds ``n_imfs``, ``error`` and the
-        ``windows``, ``sifts``, ``spacing``, ``energy`` of its IMFs."""
+        ``alloc(total)`` allocates one flat output of ``total`` samples (a NumPy array or a tensor)
+        and returns it with its pointer: every element's rows are collected into it at once, and
+        element i's (P_i, *shape_i) rows are a view of it. Returns (rows, info) per element; info
+        holds ``n_imfs``, ``error`` and the ``windows``, ``sifts``, ``spacing``, ``energy`` of its IMFs."""
         count = len(ptrs)
         dim = len(shapes[0]) if count else 1
         p = _Params(int(max_imf), -1.0 if tie_tolerance is None else float(tie_tolerance), int(sifts),
@@ -321,7 +323,7 @@ class Core:
         code = 0 if np.dtype(dtype) == np.float32 else 1
         self._check(self._lib.eda_decompose_ragged(xs, int(on_device), code, dim, count, n, ctypes.byref(p),
                                                    int(workers), ctypes.c_void_p(stream), ctypes.byref(run)))
-        out = []
+        infos, rows_of = [], []
         try:
             for i in range(count):
                 P, k, err = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
@@ -331,16 +333,23 @@ class Core:
                 info = {"n_imfs": int(k.value), "error": int(err.value), "windows": np.zeros(K, np.int32),
                         "sifts": np.zeros(K, np.int32), "spacing": np.zeros(K, np.float64),
                         "energy": np.zeros(K, np.float64)}
-                self._check(self._lib.eda_ragged_element(
-                    run, i, None, None, None, *(ctypes.c_void_p(info[f].ctypes.data) for f in
-                                                ("windows", "sifts", "spacing", "energy"))))
-                rows, ptr = out_of(P.value, tuple(shapes[i]))
-                self._check(self._lib.eda_ragged_collect(run, i, ctypes.c_void_p(ptr), int(on_device),
-                                                         ctypes.c_void_p(stream)))
-                out.append((rows, info))
+                if K:
+                    self._check(self._lib.eda_ragged_element(
+                        run, i, None, None, None, *(ctypes.c_void_p(info[f].ctypes.data) for f in
+                                                    ("windows", "sifts", "spacing", "energy"))))
+                infos.append(info)
+                rows_of.append(int(P.value))
+            sizes = [P * int(np.prod(sh)) for P, sh in zip(rows_of, shapes)]
+            offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64) if count else np.zeros(1, np.int64)
+            buf, ptr = alloc(int(offsets[-1]))
+            if count:
+                self._check(self._lib.eda_ragged_collect_all(
+                    run, ctypes.c_void_p(ptr), int(on_device), offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                    ctypes.c_void_p(stream)))
         finally:
             self._lib.eda_ragged_free(run)
-        return out
+        return [(buf[int(offsets[i]):int(offsets[i + 1])].reshape((rows_of[i],) + tuple(shapes[i])), infos[i])
+                for i in range(count)]
 
 
     def monogenic(self, ptr: int, on_device: bool, dtype: str, shape: tuple[int, ...], stream: int, out_ptr: int,

@@ -160,6 +160,12 @@ EDA_API int eda_ragged_element(const eda_ragged_run* run, int64_t i, int32_t* ro
 /* Element i's rows (P, *n_i) into dst (host, or device memory of the run's device), complete on
  * return: a NaN row for a failed element, the IMFs then the residue otherwise. */
 EDA_API int eda_ragged_collect(eda_ragged_run* run, int64_t i, void* dst, int dst_on_device, void* stream);
+/* Every element's rows at once (no counterpart in the reference): element i's (P_i, *n_i) rows into
+ * dst + offsets[i] (offsets in samples of the run's dtype; dst on the host, or device memory of the
+ * run's device, large enough for every element), complete on return. One device pass per group of
+ * the run instead of one collect per element. */
+EDA_API int eda_ragged_collect_all(eda_ragged_run* run, void* dst, int dst_on_device, const int64_t* offsets,
+                                   void* stream);
 EDA_API void eda_ragged_free(eda_ragged_run* run);
 
 /* The calling thread's last error message (NUL-terminated, truncated to len). Returns its full
