@@ -249,6 +249,32 @@ __device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t digit, bool
   if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[digit], static_cast<uint32_t>(__popc(same)));
 }
 
+// The candidates of a selection: the keys that share the digit the first pass resolved (written
+// while the second pass counts; the items of one binade slice of the element's values), which every
+// later pass reads instead of the items. cap keys per element; a selection with more candidates
+// reads the items in every pass (the count n keeps growing past cap, nothing is written there).
+template <class K>
+struct SelCand {
+  K* keys;               // [B][cap]; nullptr: no candidates
+  unsigned long long* n;  // [B]
+  int64_t cap;
+};
+// Appends key k of the lanes with app set (the warp's 32 lanes call it together).
+template <class K>
+__device__ __forceinline__ void cand_append(const SelCand<K>& c, int64_t b, bool app, K k) {
+  const unsigned m = __ballot_sync(0xffffffffu, app);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  const int first = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == first) base = atomicAdd(c.n + b, static_cast<unsigned long long>(__popc(m)));
+  base = __shfl_sync(0xffffffffu, base, first);
+  if (app) {
+    const unsigned long long pos = base + static_cast<unsigned long long>(__popc(m & ((1u << lane) - 1u)));
+    if (pos < static_cast<unsigned long long>(c.cap)) c.keys[b * c.cap + static_cast<int64_t>(pos)] = k;
+  }
+}
+
 template <class K>
 struct SelLeader {
   K prefix[2];
@@ -317,7 +343,7 @@ __device__ __forceinline__ double linear_between(double lo, double hi, double fr
 
 template <class T, class K>
 __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a, const int32_t* run, double q,
-                                                          double* out, int64_t* count_out) {
+                                                          double* out, int64_t* count_out, SelCand<K> cand) {
   constexpr int kKeyBits = 8 * static_cast<int>(sizeof(K));
   constexpr int kDigits = (kKeyBits + kDigitBits - 1) / kDigitBits;
   extern __shared__ __align__(16) unsigned char sel_smem[];
@@ -342,8 +368,11 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
       lead.prefix[0] = lead.prefix[1] = K(0);
       lead.live = 1;
       lead.same = 1;
+      if (cand.keys) cand.n[b] = 0ULL;
     }
   }
+  bool from_cand = false;
+  int64_t n_it = a.items;
   for (int pass = 0; pass < kDigits; ++pass) {
     const int hi = kKeyBits - kDigitBits * pass;  // key bits at and above hi are resolved
     const int shift = hi > kDigitBits ? hi - kDigitBits : 0;
@@ -355,17 +384,29 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
     if (!live) break;
     const bool two = pass > 0 && !L->same;
     const K p0 = L->prefix[0], p1 = L->prefix[1];
+    if (pass == 2 && cand.keys) {  // the second pass's candidates are complete (the barrier above)
+      const unsigned long long nc = *reinterpret_cast<volatile unsigned long long*>(cand.n + b);
+      from_cand = nc <= static_cast<unsigned long long>(cand.cap);
+      if (from_cand) n_it = static_cast<int64_t>(nc);
+    }
     const int64_t stride = static_cast<int64_t>(ctas) * kThreads;
     // the warp steps through the items together (count_digit is warp-collective)
-    const int64_t t_end = (a.items + 31) / 32 * 32;
+    const int64_t t_end = (n_it + 31) / 32 * 32;
     for (int64_t t = static_cast<int64_t>(me) * kThreads + tid; t < t_end + stride; t += stride) {
-      if (t - tid % 32 >= a.items) break;  // the warp's first item is past the end: the whole warp leaves
+      if (t - tid % 32 >= n_it) break;  // the warp's first item is past the end: the whole warp leaves
       K k = K(0);
-      const bool have = t < a.items && sel_key_of<T, K>(g, a, b, t, &k);
+      bool have;
+      if (from_cand) {
+        have = t < n_it;
+        if (have) k = cand.keys[b * cand.cap + t];
+      } else {
+        have = t < a.items && sel_key_of<T, K>(g, a, b, t, &k);
+      }
       const uint32_t digit = static_cast<uint32_t>((k >> shift) & dmask);
       const K top = pass == 0 ? K(0) : (k >> hi);
       count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
       if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
+      if (pass == 1 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
     }
     __syncthreads();
     const int bins = 1 << width;
@@ -452,7 +493,8 @@ __device__ __forceinline__ void digit_of_pass(int pass, int* hi, int* shift, int
 template <class T, class K>
 __global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T> a, const int32_t* run,
                                                              const SelGridState<K>* st,
-                                                             unsigned long long* table, int32_t pass) {
+                                                             unsigned long long* table, int32_t pass,
+                                                             SelCand<K> cand) {
   __shared__ uint32_t local[2 * kDigitBins];
   const int64_t b = blockIdx.y;
   if (run && !run[b]) return;
@@ -470,15 +512,30 @@ __global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T>
   const int tid = threadIdx.x;
   for (int i = tid; i < 2 * kDigitBins; i += kThreads) local[i] = 0u;
   __syncthreads();
+  // from the third pass on, the second pass's candidates (when they fit) instead of the items
+  bool from_cand = false;
+  int64_t n_it = a.items;
+  if (pass >= 2 && cand.keys) {
+    const unsigned long long nc = cand.n[b];
+    from_cand = nc <= static_cast<unsigned long long>(cand.cap);
+    if (from_cand) n_it = static_cast<int64_t>(nc);
+  }
   const int64_t stride = static_cast<int64_t>(gridDim.x) * kThreads;
   for (int64_t t = static_cast<int64_t>(blockIdx.x) * kThreads + tid;; t += stride) {
-    if (t - tid % 32 >= a.items) break;  // the warp's first item is past the end
+    if (t - tid % 32 >= n_it) break;  // the warp's first item is past the end
     K k = K(0);
-    const bool have = t < a.items && sel_key_of<T, K>(g, a, b, t, &k);
+    bool have;
+    if (from_cand) {
+      have = t < n_it;
+      if (have) k = cand.keys[b * cand.cap + t];
+    } else {
+      have = t < a.items && sel_key_of<T, K>(g, a, b, t, &k);
+    }
     const uint32_t digit = static_cast<uint32_t>((k >> shift) & dmask);
     const K top = pass == 0 ? K(0) : (k >> hi);
     count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
     if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
+    if (pass == 1 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
   }
   __syncthreads();
   const int bins = 1 << width;
@@ -586,9 +643,27 @@ void field_totals(cudaStream_t s, const Geom& g, const T* f, double* energy, dou
   EDAB_LAUNCH("element_totals");
 }
 
+// Candidate keys per element: a quarter of the largest selection's items (the differences along
+// every axis), at least 64.
+int64_t cand_cap(const Geom& g) { return std::max<int64_t>(64, static_cast<int64_t>(g.dim) * g.field / 4 / 32 * 32); }
+
+// scratch: the grid form's states and count tables, then the candidates' counts and keys
 size_t select_scratch_bytes(const Geom& g) {
-  return align256(static_cast<size_t>(g.batch) * sizeof(SelGridState<uint64_t>)) +
-         align256(static_cast<size_t>(g.batch) * 2 * kDigitBins * sizeof(unsigned long long));
+  const size_t B = static_cast<size_t>(g.batch);
+  return align256(B * sizeof(SelGridState<uint64_t>)) + align256(B * 2 * kDigitBins * sizeof(unsigned long long)) +
+         align256(B * sizeof(unsigned long long)) + align256(B * static_cast<size_t>(cand_cap(g)) * sizeof(uint64_t));
+}
+
+template <class K>
+SelCand<K> cand_of(const Geom& g, void* scratch) {
+  const size_t B = static_cast<size_t>(g.batch);
+  char* p = static_cast<char*>(scratch) + align256(B * sizeof(SelGridState<uint64_t>)) +
+            align256(B * 2 * kDigitBins * sizeof(unsigned long long));
+  SelCand<K> c;
+  c.n = reinterpret_cast<unsigned long long*>(p);
+  c.keys = reinterpret_cast<K*>(p + align256(B * sizeof(unsigned long long)));
+  c.cap = cand_cap(g);
+  return c;
 }
 
 // The grid-wide form: every digit a counting and a pick launch (scratch: the states, then the
@@ -607,8 +682,11 @@ void select_grid(cudaStream_t s, const Geom& g, const SelView<T>& a, double q, c
   const int64_t fill = std::min<int64_t>((int64_t{8} * sms + g.batch - 1) / g.batch,
                                          std::max<int64_t>(1, a.items / (int64_t{kThreads} * 4)));
   const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>(std::max(by_items, fill), 1, 1024));
+  const SelCand<K> cand = cand_of<K>(g, scratch);
+  EDAB_CUDA(cudaMemsetAsync(cand.n, 0, static_cast<size_t>(g.batch) * sizeof(unsigned long long), s));
   for (int pass = 0; pass < kDigits; ++pass) {
-    select_grid_count<T, K><<<dim3(ctas, static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(g, a, run, st, table, pass);
+    select_grid_count<T, K><<<dim3(ctas, static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(g, a, run, st, table, pass,
+                                                                                          cand);
     EDAB_LAUNCH("select_grid_count");
     select_grid_pick<K><<<static_cast<unsigned>(g.batch), kThreads, 0, s>>>(run, st, table, pass, q, out, count);
     EDAB_LAUNCH("select_grid_pick");
@@ -663,20 +741,20 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const auto launch = [&](auto kernel) {
+  const auto launch = [&](auto kernel, auto cand) {
     once_on_device(reinterpret_cast<const void*>(kernel), [&] {
       EDAB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSelSmem)));
     });
-    EDAB_CUDA(cudaLaunchKernelEx(&cfg, kernel, g, a, run, q, out, count));
+    EDAB_CUDA(cudaLaunchKernelEx(&cfg, kernel, g, a, run, q, out, count, cand));
     EDAB_LAUNCH("select_cluster");
   };
   if constexpr (std::is_same_v<T, float>) {
     if (sel.center == nullptr) {
-      launch(select_cluster<T, uint32_t>);
+      launch(select_cluster<T, uint32_t>, scratch ? cand_of<uint32_t>(g, scratch) : SelCand<uint32_t>{});
       return;
     }
   }
-  launch(select_cluster<T, uint64_t>);
+  launch(select_cluster<T, uint64_t>, scratch ? cand_of<uint64_t>(g, scratch) : SelCand<uint64_t>{});
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -294,3 +294,29 @@ def test_select_in_clusters(dev, dtype, shape):
                 want = oracle.select(v, q)
                 assert (np.isnan(out[b]) and np.isnan(want)) or out[b] == want, (kw, q, b)
                 assert cnt[b] == v.size
+
+
+# From the third digit on, a selection reads the second pass's candidates (the keys that share the
+# first digit) when they fit a quarter of the items, else the items again: a constant field and a
+# field of one binade overflow the candidates, a field of many binades does not. Both forms.
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("batch", [2, 40])
+def test_select_candidates_and_their_overflow(dev, dtype, batch):
+    rng = np.random.default_rng(batch)
+    shape = (batch, 96, 80)
+    fields = {
+        "constant": np.full(shape, 1.25),
+        "one binade": 1.0 + rng.random(shape),
+        "many binades": rng.standard_normal(shape) * np.exp(rng.uniform(-30, 30, shape)),
+    }
+    center = rng.standard_normal(batch)
+    for name, x in fields.items():
+        x = x.astype(dtype)
+        for kw in ({}, {"center": center}, {"src": 1, "axes": 3}):
+            for q in (-1.0, 0.75):
+                out, cnt = gpu_select(dev, x, q=q, **kw)
+                for b in range(batch):
+                    v = items(x[b], kw.get("src", 0), kw.get("axes", 0), None, 0,
+                              None if "center" not in kw else center[b])
+                    assert out[b] == oracle.select(v, q), (name, kw, q, b)
+                    assert cnt[b] == v.size
