@@ -428,8 +428,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   const T idn = fold_identity<T, OP>();
   if (q.wa == 1) {
     // one-sample segments: H = G = the sample, so y = op(v, v): the sample for max / min, and for
-    // sums the aligned mean (v + v) * 0.5 of the canonical path, rounded the same way
-    for (int32_t i = worker; i < n; i += workers) {
+    // sums the aligned mean (v + v) * 0.5 of the canonical path, rounded the same way. With r = 0
+    // and o = 0 the G segments are the outputs themselves: the whole line, or a long line's tile.
+    const int32_t i1 = q.o + q.k_lo + q.gk0 + q.gn;
+    for (int32_t i = q.o + q.k_lo + q.gk0 + worker; i < i1; i += workers) {
       const T v = Vp[i * PP];
       Rp[i * PP] = OP == kOpSum ? mul_rn(add_rn(v, v), T(0.5)) : v;
     }
