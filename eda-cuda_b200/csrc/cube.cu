@@ -1008,7 +1008,13 @@ __global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a,
   const int32_t nv = vhi - vlo + 1, nx = xhi - xlo + 1;
   const int32_t TS = max(t.gn, t.hn) * q.cps;
   const int32_t nv16 = (nv + 3) & ~3, nx16 = (nx + 3) & ~3;  // 16-byte aligned regions
-  const bool tiled = nv16 + nx16 + 2 * TS <= smem_elems;
+  // Every tile of the line decides alike (a tile that folded alone beside a whole-line fold would
+  // rewrite the outputs that fold works in): by bounds of any tile's samples, slots and totals
+  // (nv, nx <= L + 2r + 2wa + 4, TS <= ((L + 2wa) / wa + 2) cps, checked against every tile's
+  // exact extents on the CPU).
+  const int32_t span16 = (kLongTile + 2 * q.r + 2 * q.wa + 4 + 3) & ~3;
+  const int32_t ts_bound = ((kLongTile + 2 * q.wa) / q.wa + 2) * q.cps;
+  const bool tiled = 2 * span16 + 2 * ts_bound <= smem_elems && nv16 + nx16 + 2 * TS <= smem_elems;
   if (!tiled && blockIdx.x != 0) return;  // the whole line folds in the tile-0 CTA
   __syncthreads();
   const T* line = keys + b * g.pitch;
