@@ -414,9 +414,12 @@ struct Tasks {
 
 // One stage on the staged lines of this CTA: V -> R (sample i of line p at p LS + i PP), tot: the
 // chunk totals / carries [2][TS][P] (slot k cps + c). Workers: P lanes each (lane % P = the line).
-template <class T, int OP, int P, int PP>
+// RANGE: fold the window's segment range (a long line's tile); else every segment of the line.
+template <class T, int OP, int P, int PP, bool RANGE = false>
 __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict__ R, T* __restrict__ tot, int32_t n,
                                           int32_t TS, const Win& q, int32_t LS, int32_t seq_share) {
+  const int32_t hn = RANGE ? q.hn : q.nseg, gn = RANGE ? q.gn : q.nseg;
+  const int32_t hk0 = RANGE ? q.hk0 : 0, gk0 = RANGE ? q.gk0 : 0;
   constexpr int slots = 32 / P;
   constexpr int workers = kWarps * slots;
   const int lane = threadIdx.x & 31;
@@ -430,8 +433,8 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     // one-sample segments: H = G = the sample, so y = op(v, v): the sample for max / min, and for
     // sums the aligned mean (v + v) * 0.5 of the canonical path, rounded the same way. With r = 0
     // and o = 0 the G segments are the outputs themselves: the whole line, or a long line's tile.
-    const int32_t i1 = q.o + q.k_lo + q.gk0 + q.gn;
-    for (int32_t i = q.o + q.k_lo + q.gk0 + worker; i < i1; i += workers) {
+    const int32_t i1 = q.o + q.k_lo + gk0 + gn;
+    for (int32_t i = q.o + q.k_lo + gk0 + worker; i < i1; i += workers) {
       const T v = Vp[i * PP];
       Rp[i * PP] = OP == kOpSum ? mul_rn(add_rn(v, v), T(0.5)) : v;
     }
@@ -443,11 +446,11 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   // phases. Windows of few, long segments (seq_share * nseg < workers) split their segments into
   // chunks over the workers instead: chunk totals, carries, then the H and G folds (four phases,
   // twice the folds, but every worker busy).
-  if (q.cps == 1 || max(q.hn, q.gn) * seq_share >= workers) {
-    const int32_t hper = (q.hn + workers - 1) / workers;
-    const int32_t hk_end = min((worker + 1) * hper, q.hn);
+  if (q.cps == 1 || max(hn, gn) * seq_share >= workers) {
+    const int32_t hper = (hn + workers - 1) / workers;
+    const int32_t hk_end = min((worker + 1) * hper, hn);
     for (int32_t k = worker * hper; k < hk_end; ++k) {
-      const int32_t s = q.o + (q.k_lo + q.hk0 + k) * q.wa;
+      const int32_t s = q.o + (q.k_lo + hk0 + k) * q.wa;
       const int32_t c1 = min(s + q.wa - 1, e_max);
       if (q.cps > 1) {
         seg_h<T, OP, PP>(Vp, Rp, n, q, s, c1);
@@ -460,10 +463,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
       }
     }
     __syncthreads();
-    const int32_t gper = (q.gn + workers - 1) / workers;
-    const int32_t gk_end = min((worker + 1) * gper, q.gn);
+    const int32_t gper = (gn + workers - 1) / workers;
+    const int32_t gk_end = min((worker + 1) * gper, gn);
     for (int32_t k = worker * gper; k < gk_end; ++k) {
-      const int32_t s = q.o + (q.k_lo + q.gk0 + k) * q.wa;
+      const int32_t s = q.o + (q.k_lo + gk0 + k) * q.wa;
       const int32_t e_al = s + q.wa - 1;
       const int32_t c1 = min(e_al, e_max);
       if (q.cps > 1) {
@@ -492,8 +495,8 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     // phase 1: chunk totals; half of the workers take the line, half the reversed line
     constexpr int half = workers / 2;
     const int dir = worker >= half;
-    const int32_t dn = dir ? q.hn : q.gn;
-    const int32_t dk0 = q.k_lo + (dir ? q.hk0 : q.gk0);
+    const int32_t dn = dir ? hn : gn;
+    const int32_t dk0 = q.k_lo + (dir ? hk0 : gk0);
     for (Tasks t(worker - dir * half, half, dn); t.c < q.cps; t.next(dn)) {
       const int32_t s = q.o + (dk0 + t.k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
@@ -516,10 +519,10 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     }
     __syncthreads();
     // phase 2: exclusive carries per segment, in place (slot c holds the carry of chunk c >= 1)
-    for (int32_t t = worker; t < q.gn + q.hn; t += workers) {
-      const int dir = t >= q.gn;
-      const int32_t k = t - dir * q.gn;
-      const int32_t s = q.o + (q.k_lo + (dir ? q.hk0 : q.gk0) + k) * q.wa;
+    for (int32_t t = worker; t < gn + hn; t += workers) {
+      const int dir = t >= gn;
+      const int32_t k = t - dir * gn;
+      const int32_t s = q.o + (q.k_lo + (dir ? hk0 : gk0) + k) * q.wa;
       const int32_t e_last = min(s + q.wa - 1, e_max);
       const int32_t nch = (e_last - s) / 32 + 1;
       T* tl = tot + (dir * TS + k * q.cps) * P + p;
@@ -533,8 +536,8 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
     __syncthreads();
   }
   // phase 3: H (the reversed line's G) into R at the output slots n - 1 + r - e (e >= r)
-  for (Tasks t(worker, workers, q.hn); t.c < q.cps; t.next(q.hn)) {
-    const int32_t s = q.o + (q.k_lo + q.hk0 + t.k) * q.wa;
+  for (Tasks t(worker, workers, hn); t.c < q.cps; t.next(hn)) {
+    const int32_t s = q.o + (q.k_lo + hk0 + t.k) * q.wa;
     const int32_t e_last = min(s + q.wa - 1, e_max);
     const int32_t c0 = s + 32 * t.c;
     if (c0 > e_last) continue;
@@ -553,8 +556,8 @@ __device__ __forceinline__ void run_stage(const T* __restrict__ V, T* __restrict
   }
   __syncthreads();
   // phase 4: G combined with H in place: y(x) = op(H(x - r), G(x + r)), slot x = e - r
-  for (Tasks t(worker, workers, q.gn); t.c < q.cps; t.next(q.gn)) {
-    const int32_t s = q.o + (q.k_lo + q.gk0 + t.k) * q.wa;
+  for (Tasks t(worker, workers, gn); t.c < q.cps; t.next(gn)) {
+    const int32_t s = q.o + (q.k_lo + gk0 + t.k) * q.wa;
     const int32_t e_al = s + q.wa - 1;
     const int32_t e_last = min(e_al, e_max);
     const int32_t c0 = s + 32 * t.c;
@@ -1028,9 +1031,9 @@ __global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a,
     for (int f = 0; f < nf; ++f) {
       const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
       // (the staged samples and slots at their line indices: only the staged ones are touched)
-      if (box) run_stage<T, kOpSum, 1, 1>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
-      else if (is_min) run_stage<T, kOpMinK, 1, 1>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
-      else run_stage<T, kOpMaxK, 1, 1>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+      if (box) run_stage<T, kOpSum, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+      else if (is_min) run_stage<T, kOpMinK, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+      else run_stage<T, kOpMaxK, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
       T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
       const T* aux = detsq ? a.aux + b * g.field : nullptr;
       const int32_t end = X1 == n ? static_cast<int32_t>(g.pitch) : X1;  // the last tile writes the pads

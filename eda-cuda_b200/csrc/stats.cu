@@ -249,10 +249,12 @@ __device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t digit, bool
   if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[digit], static_cast<uint32_t>(__popc(same)));
 }
 
-// The candidates of a selection: the keys that share the digit the first pass resolved (written
-// while the second pass counts; the items of one binade slice of the element's values), which every
-// later pass reads instead of the items. cap keys per element; a selection with more candidates
-// reads the items in every pass (the count n keeps growing past cap, nothing is written there).
+// The candidates of a 64-bit selection: the keys that share the two digits the first two passes
+// resolved (written while the third pass counts: the items within about 2^-10 of the statistic's
+// binade position, a small slice of the element), which the last three passes read instead of the
+// items. cap keys per element; a selection with more candidates reads the items in every pass (the
+// count n keeps growing past cap, nothing is written there). 32-bit selections (three digits) have
+// no pass after the third and take none.
 template <class K>
 struct SelCand {
   K* keys;               // [B][cap]; nullptr: no candidates
@@ -384,7 +386,7 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
     if (!live) break;
     const bool two = pass > 0 && !L->same;
     const K p0 = L->prefix[0], p1 = L->prefix[1];
-    if (pass == 2 && cand.keys) {  // the second pass's candidates are complete (the barrier above)
+    if (pass == 3 && cand.keys) {  // the third pass's candidates are complete (the barrier above)
       const unsigned long long nc = *reinterpret_cast<volatile unsigned long long*>(cand.n + b);
       from_cand = nc <= static_cast<unsigned long long>(cand.cap);
       if (from_cand) n_it = static_cast<int64_t>(nc);
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
       const K top = pass == 0 ? K(0) : (k >> hi);
       count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
       if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
-      if (pass == 1 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
+      if (pass == 2 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
     }
     __syncthreads();
     const int bins = 1 << width;
@@ -512,10 +514,10 @@ __global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T>
   const int tid = threadIdx.x;
   for (int i = tid; i < 2 * kDigitBins; i += kThreads) local[i] = 0u;
   __syncthreads();
-  // from the third pass on, the second pass's candidates (when they fit) instead of the items
+  // from the fourth pass on, the third pass's candidates (when they fit) instead of the items
   bool from_cand = false;
   int64_t n_it = a.items;
-  if (pass >= 2 && cand.keys) {
+  if (pass >= 3 && cand.keys) {
     const unsigned long long nc = cand.n[b];
     from_cand = nc <= static_cast<unsigned long long>(cand.cap);
     if (from_cand) n_it = static_cast<int64_t>(nc);
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T>
     const K top = pass == 0 ? K(0) : (k >> hi);
     count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
     if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
-    if (pass == 1 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
+    if (pass == 2 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
   }
   __syncthreads();
   const int bins = 1 << width;
@@ -682,8 +684,8 @@ void select_grid(cudaStream_t s, const Geom& g, const SelView<T>& a, double q, c
   const int64_t fill = std::min<int64_t>((int64_t{8} * sms + g.batch - 1) / g.batch,
                                          std::max<int64_t>(1, a.items / (int64_t{kThreads} * 4)));
   const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>(std::max(by_items, fill), 1, 1024));
-  const SelCand<K> cand = cand_of<K>(g, scratch);
-  EDAB_CUDA(cudaMemsetAsync(cand.n, 0, static_cast<size_t>(g.batch) * sizeof(unsigned long long), s));
+  const SelCand<K> cand = sizeof(K) == 8 ? cand_of<K>(g, scratch) : SelCand<K>{};
+  if (cand.keys) EDAB_CUDA(cudaMemsetAsync(cand.n, 0, static_cast<size_t>(g.batch) * sizeof(unsigned long long), s));
   for (int pass = 0; pass < kDigits; ++pass) {
     select_grid_count<T, K><<<dim3(ctas, static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(g, a, run, st, table, pass,
                                                                                           cand);
@@ -750,7 +752,7 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
   };
   if constexpr (std::is_same_v<T, float>) {
     if (sel.center == nullptr) {
-      launch(select_cluster<T, uint32_t>, scratch ? cand_of<uint32_t>(g, scratch) : SelCand<uint32_t>{});
+      launch(select_cluster<T, uint32_t>, SelCand<uint32_t>{});
       return;
     }
   }

@@ -296,9 +296,10 @@ def test_select_in_clusters(dev, dtype, shape):
                 assert cnt[b] == v.size
 
 
-# From the third digit on, a selection reads the second pass's candidates (the keys that share the
-# first digit) when they fit a quarter of the items, else the items again: a constant field and a
-# field of one binade overflow the candidates, a field of many binades does not. Both forms.
+# From the fourth digit on, a 64-bit selection (float64 items, or centred ones) reads the third
+# pass's candidates (the keys that share the first two digits) when they fit a quarter of the
+# items, else the items again: a constant field overflows the candidates, fields of one or many
+# binades do not. Both forms.
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("batch", [2, 40])
 def test_select_candidates_and_their_overflow(dev, dtype, batch):
