@@ -308,6 +308,7 @@ int eda_release_workspace(void) {
   return guarded([&] {
     edab::thread_workspace().release();
     edab::thread_staging().release();
+    edab::release_leased_workspaces();
   });
 }
 

@@ -48,9 +48,44 @@ void Workspace::reserve(size_t bytes, cudaStream_t s) {
   device_ = dev;
 }
 
+namespace {
+thread_local Workspace* t_leased = nullptr;
+std::mutex g_pool_mu;
+std::vector<std::unique_ptr<Workspace>>& idle_workspaces() {
+  static std::vector<std::unique_ptr<Workspace>> v;
+  return v;
+}
+}  // namespace
+
 Workspace& thread_workspace() {
   thread_local Workspace ws;
-  return ws;
+  return t_leased ? *t_leased : ws;
+}
+
+void set_thread_workspace(Workspace* ws) { t_leased = ws; }
+
+Workspace* lease_workspace() {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  auto& v = idle_workspaces();
+  if (v.empty()) return new Workspace();
+  Workspace* w = v.back().release();
+  v.pop_back();
+  return w;
+}
+
+void return_workspace(Workspace* ws) {
+  if (!ws) return;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  idle_workspaces().emplace_back(ws);
+}
+
+void release_leased_workspaces() {
+  std::vector<std::unique_ptr<Workspace>> v;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    v.swap(idle_workspaces());
+  }
+  for (auto& w : v) w->release();
 }
 
 HostStaging::~HostStaging() { release(); }

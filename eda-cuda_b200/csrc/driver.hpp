@@ -41,7 +41,15 @@ class Workspace {
   int device_ = -1;
   bool owned_ = true;
 };
+// The calling thread's workspace: its own, or the one it leases (set_thread_workspace).
 Workspace& thread_workspace();
+void set_thread_workspace(Workspace* ws);  // nullptr: the thread's own again
+// Workspaces of ragged-batch workers, kept across calls: a worker thread lives for one call, and a
+// workspace of its own would be allocated on every call and freed when the thread ends (cudaFree
+// synchronises the device, so the workers' ends would wait for one another's work).
+Workspace* lease_workspace();
+void return_workspace(Workspace* ws);
+void release_leased_workspaces();  // frees the idle ones
 
 // Pinned host memory of the calling thread for device-to-host copies into pageable memory: two
 // pieces of kPiece bytes, allocated on first use and kept until released.

@@ -182,6 +182,8 @@ std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_devic
   RaggedRun* res = out.get();
   auto work = [&] {
     cudaStream_t ws = nullptr;
+    Workspace* leased = nw > 1 ? lease_workspace() : nullptr;  // one worker: the caller's own
+    if (leased) set_thread_workspace(leased);
     try {
       EDAB_CUDA(cudaSetDevice(device));
       EDAB_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
@@ -202,6 +204,10 @@ std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_devic
     if (ws) {
       cudaStreamSynchronize(ws);
       cudaStreamDestroy(ws);
+    }
+    if (leased) {
+      set_thread_workspace(nullptr);
+      return_workspace(leased);
     }
   };
   if (nw == 1) {
