@@ -124,11 +124,12 @@ def test_ragged_rejects_a_field_beyond_the_axis_limit(torch):
 
 
 def test_fresh_workspaces_are_zeroed_on_the_workers_streams(torch):
-    """Each ragged call starts new worker threads, whose workspaces are allocated and zeroed anew.
-    With the caller on a non-blocking stream and the legacy default stream kept busy by other work,
-    a zeroing queued on the legacy stream would land in the middle of the workers' kernels (which
-    run on their own non-blocking streams) and corrupt their inputs; zeroed on the workers' own
-    streams, every field must still equal its one-field call."""
+    """Each ragged call starts new worker threads, which lease workspaces (allocated and zeroed when
+    the pool has none idle; released here first). With the caller on a non-blocking stream and the
+    legacy default stream kept busy by other work, a zeroing queued on the legacy stream would land
+    in the middle of the workers' kernels (which run on their own non-blocking streams) and corrupt
+    their inputs; zeroed on the workers' own streams, every field must still equal its one-field
+    call."""
     import eda
 
     xs = [signal(400, 11), signal(400, 13), signal(520, 12), signal(520, 14)]
@@ -138,6 +139,7 @@ def test_fresh_workspaces_are_zeroed_on_the_workers_streams(torch):
     a = torch.randn(8192, 8192, device="cuda")
     for _ in range(3):
         torch.cuda.synchronize()
+        assert eda._native.core()._lib.eda_release_workspace() == 0  # fresh workspaces for the workers
         busy = a
         for _ in range(24):  # tens of milliseconds of work on the legacy default stream
             busy = busy @ a
