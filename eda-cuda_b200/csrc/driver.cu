@@ -11,6 +11,8 @@
 #include <mutex>
 #include <thread>
 
+#include <sys/mman.h>
+
 namespace edab {
 
 Workspace::~Workspace() { release(); }
@@ -104,9 +106,44 @@ void HostStaging::release() {
   base_ = nullptr;
 }
 
+namespace {
+thread_local HostStaging* t_leased_staging = nullptr;
+std::mutex g_staging_mu;
+std::vector<std::unique_ptr<HostStaging>>& idle_stagings() {
+  static std::vector<std::unique_ptr<HostStaging>> v;
+  return v;
+}
+}  // namespace
+
 HostStaging& thread_staging() {
   thread_local HostStaging st;
-  return st;
+  return t_leased_staging ? *t_leased_staging : st;
+}
+
+void set_thread_staging(HostStaging* st) { t_leased_staging = st; }
+
+HostStaging* lease_staging() {
+  std::lock_guard<std::mutex> lock(g_staging_mu);
+  auto& v = idle_stagings();
+  if (v.empty()) return new HostStaging();
+  HostStaging* h = v.back().release();
+  v.pop_back();
+  return h;
+}
+
+void return_staging(HostStaging* st) {
+  if (!st) return;
+  std::lock_guard<std::mutex> lock(g_staging_mu);
+  idle_stagings().emplace_back(st);
+}
+
+void release_leased_stagings() {
+  std::vector<std::unique_ptr<HostStaging>> v;
+  {
+    std::lock_guard<std::mutex> lock(g_staging_mu);
+    v.swap(idle_stagings());
+  }
+  for (auto& h : v) h->release();
 }
 
 namespace {
@@ -132,6 +169,15 @@ void parallel_memcpy(unsigned char* dst, const unsigned char* src, size_t bytes,
 
 void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return;
+  // A large destination not touched yet (a fresh output array) takes a page fault per 4 KiB page
+  // during the copy: ask for huge pages on its whole 2 MiB pages first (a hint on this process's
+  // own mapping; ignored where the kernel does not support it).
+  if (bytes >= (size_t{8} << 20)) {
+    const uintptr_t huge = uintptr_t{2} << 20;
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(dst) + huge - 1) & ~(huge - 1);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(dst) + bytes) & ~(huge - 1);
+    if (e > a) (void)madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+  }
   HostStaging& st = thread_staging();
   const unsigned threads = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
   const size_t P = HostStaging::kPiece;
@@ -152,6 +198,33 @@ void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) 
     const size_t off = i * P, len = std::min(P, bytes - off);
     parallel_memcpy(static_cast<unsigned char*>(dst) + off, st.piece(static_cast<int>(i & 1)), len, threads);
   }
+  cudaEventDestroy(done[0]);
+  cudaEventDestroy(done[1]);
+}
+
+void copy_from_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return;
+  if (bytes < (size_t{4} << 20)) {  // small: the driver's own staging (src is free on return)
+    EDAB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    return;
+  }
+  HostStaging& st = thread_staging();
+  const unsigned threads = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const size_t P = HostStaging::kPiece;
+  const size_t pieces = (bytes + P - 1) / P;
+  cudaEvent_t done[2];
+  EDAB_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+  EDAB_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+  for (size_t i = 0; i < pieces; ++i) {
+    const size_t off = i * P, len = std::min(P, bytes - off);
+    unsigned char* piece = st.piece(static_cast<int>(i & 1));
+    if (i >= 2) EDAB_CUDA(cudaEventSynchronize(done[i & 1]));  // the piece's previous transfer is done
+    parallel_memcpy(piece, static_cast<const unsigned char*>(src) + off, len, threads);
+    EDAB_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, piece, len, cudaMemcpyHostToDevice, s));
+    EDAB_CUDA(cudaEventRecord(done[i & 1], s));
+  }
+  // the pieces are free for the thread's next copy
+  EDAB_CUDA(cudaEventSynchronize(done[(pieces - 1) & 1]));
   cudaEventDestroy(done[0]);
   cudaEventDestroy(done[1]);
 }
@@ -578,8 +651,9 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
       else convert_chunk<double>(s, *src, x, b0, nb, dim, n, static_cast<double*>(staged));
     } else {
       const unsigned char* in = static_cast<const unsigned char*>(x) + static_cast<size_t>(b0) * g.count * es;
-      EDAB_CUDA(cudaMemcpyAsync(staged, in, static_cast<size_t>(nb) * g.count * es,
-                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+      const size_t bytes = static_cast<size_t>(nb) * g.count * es;
+      if (on_device) EDAB_CUDA(cudaMemcpyAsync(staged, in, bytes, cudaMemcpyDeviceToDevice, s));
+      else copy_from_pageable(staged, in, bytes, s);
     }
     const size_t ho = static_cast<size_t>(b0) * static_cast<size_t>(cap - 1);
     unsigned char* rows0 = static_cast<unsigned char*>(run->dev_rows) + static_cast<size_t>(b0) * cap * g.count * es;

@@ -63,12 +63,20 @@ class HostStaging {
  private:
   unsigned char* base_ = nullptr;
 };
-HostStaging& thread_staging();
+HostStaging& thread_staging();  // the thread's own, or the one it leases
+void set_thread_staging(HostStaging* st);  // nullptr: the thread's own again
+// Pinned stagings of ragged-batch workers, kept across calls like their workspaces.
+HostStaging* lease_staging();
+void return_staging(HostStaging* st);
+void release_leased_stagings();  // frees the idle ones
 
 // Copies bytes from device memory src to pageable host memory dst on stream s: the transfers land
 // in the pinned pieces (double-buffered) and host threads copy each piece on while the next one
 // transfers. Returns when dst holds every byte.
 void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// The reverse: bytes of pageable host memory src into device memory dst on stream s, host threads
+// filling one pinned piece while the other transfers. src may be reused on return.
+void copy_from_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 struct Params {
   int32_t max_imf = -1;
