@@ -202,6 +202,15 @@ void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) 
   cudaEventDestroy(done[1]);
 }
 
+bool is_pinned(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 void copy_from_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return;
   if (bytes < (size_t{4} << 20)) {  // small: the driver's own staging (src is free on return)
@@ -652,8 +661,11 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
     } else {
       const unsigned char* in = static_cast<const unsigned char*>(x) + static_cast<size_t>(b0) * g.count * es;
       const size_t bytes = static_cast<size_t>(nb) * g.count * es;
-      if (on_device) EDAB_CUDA(cudaMemcpyAsync(staged, in, bytes, cudaMemcpyDeviceToDevice, s));
-      else copy_from_pageable(staged, in, bytes, s);
+      if (on_device || is_pinned(in)) {
+        EDAB_CUDA(cudaMemcpyAsync(staged, in, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+      } else {
+        copy_from_pageable(staged, in, bytes, s);
+      }
     }
     const size_t ho = static_cast<size_t>(b0) * static_cast<size_t>(cap - 1);
     unsigned char* rows0 = static_cast<unsigned char*>(run->dev_rows) + static_cast<size_t>(b0) * cap * g.count * es;

@@ -77,6 +77,8 @@ void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // The reverse: bytes of pageable host memory src into device memory dst on stream s, host threads
 // filling one pinned piece while the other transfers. src may be reused on return.
 void copy_from_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// Whether p is page-locked host memory (copied by DMA directly, not through the staging).
+bool is_pinned(const void* p);
 
 struct Params {
   int32_t max_imf = -1;
