@@ -169,6 +169,11 @@ void parallel_memcpy(unsigned char* dst, const unsigned char* src, size_t bytes,
 
 void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return;
+  if (is_pinned(dst)) {  // page-locked already: one DMA
+    EDAB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    EDAB_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
   // A large destination not touched yet (a fresh output array) takes a page fault per 4 KiB page
   // during the copy: ask for huge pages on its whole 2 MiB pages first (a hint on this process's
   // own mapping; ignored where the kernel does not support it).
