@@ -309,7 +309,6 @@ int eda_release_workspace(void) {
     edab::thread_workspace().release();
     edab::thread_staging().release();
     edab::release_leased_workspaces();
-    edab::release_leased_stagings();
   });
 }
 

@@ -106,44 +106,9 @@ void HostStaging::release() {
   base_ = nullptr;
 }
 
-namespace {
-thread_local HostStaging* t_leased_staging = nullptr;
-std::mutex g_staging_mu;
-std::vector<std::unique_ptr<HostStaging>>& idle_stagings() {
-  static std::vector<std::unique_ptr<HostStaging>> v;
-  return v;
-}
-}  // namespace
-
 HostStaging& thread_staging() {
   thread_local HostStaging st;
-  return t_leased_staging ? *t_leased_staging : st;
-}
-
-void set_thread_staging(HostStaging* st) { t_leased_staging = st; }
-
-HostStaging* lease_staging() {
-  std::lock_guard<std::mutex> lock(g_staging_mu);
-  auto& v = idle_stagings();
-  if (v.empty()) return new HostStaging();
-  HostStaging* h = v.back().release();
-  v.pop_back();
-  return h;
-}
-
-void return_staging(HostStaging* st) {
-  if (!st) return;
-  std::lock_guard<std::mutex> lock(g_staging_mu);
-  idle_stagings().emplace_back(st);
-}
-
-void release_leased_stagings() {
-  std::vector<std::unique_ptr<HostStaging>> v;
-  {
-    std::lock_guard<std::mutex> lock(g_staging_mu);
-    v.swap(idle_stagings());
-  }
-  for (auto& h : v) h->release();
+  return st;
 }
 
 namespace {
@@ -214,33 +179,6 @@ bool is_pinned(const void* p) {
     return false;
   }
   return at.type == cudaMemoryTypeHost;
-}
-
-void copy_from_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-  if (bytes == 0) return;
-  if (bytes < (size_t{4} << 20)) {  // small: the driver's own staging (src is free on return)
-    EDAB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
-    return;
-  }
-  HostStaging& st = thread_staging();
-  const unsigned threads = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  const size_t P = HostStaging::kPiece;
-  const size_t pieces = (bytes + P - 1) / P;
-  cudaEvent_t done[2];
-  EDAB_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
-  EDAB_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
-  for (size_t i = 0; i < pieces; ++i) {
-    const size_t off = i * P, len = std::min(P, bytes - off);
-    unsigned char* piece = st.piece(static_cast<int>(i & 1));
-    if (i >= 2) EDAB_CUDA(cudaEventSynchronize(done[i & 1]));  // the piece's previous transfer is done
-    parallel_memcpy(piece, static_cast<const unsigned char*>(src) + off, len, threads);
-    EDAB_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, piece, len, cudaMemcpyHostToDevice, s));
-    EDAB_CUDA(cudaEventRecord(done[i & 1], s));
-  }
-  // the pieces are free for the thread's next copy
-  EDAB_CUDA(cudaEventSynchronize(done[(pieces - 1) & 1]));
-  cudaEventDestroy(done[0]);
-  cudaEventDestroy(done[1]);
 }
 
 // The rows of the runs come from a stream-ordered pool per device that keeps up to 2 GiB cached
@@ -666,11 +604,7 @@ std::unique_ptr<Run> decompose_impl(const void* x, bool on_device, const SourceV
     } else {
       const unsigned char* in = static_cast<const unsigned char*>(x) + static_cast<size_t>(b0) * g.count * es;
       const size_t bytes = static_cast<size_t>(nb) * g.count * es;
-      if (on_device || is_pinned(in)) {
-        EDAB_CUDA(cudaMemcpyAsync(staged, in, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-      } else {
-        copy_from_pageable(staged, in, bytes, s);
-      }
+      EDAB_CUDA(cudaMemcpyAsync(staged, in, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     }
     const size_t ho = static_cast<size_t>(b0) * static_cast<size_t>(cap - 1);
     unsigned char* rows0 = static_cast<unsigned char*>(run->dev_rows) + static_cast<size_t>(b0) * cap * g.count * es;

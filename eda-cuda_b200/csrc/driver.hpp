@@ -63,20 +63,12 @@ class HostStaging {
  private:
   unsigned char* base_ = nullptr;
 };
-HostStaging& thread_staging();  // the thread's own, or the one it leases
-void set_thread_staging(HostStaging* st);  // nullptr: the thread's own again
-// Pinned stagings of ragged-batch workers, kept across calls like their workspaces.
-HostStaging* lease_staging();
-void return_staging(HostStaging* st);
-void release_leased_stagings();  // frees the idle ones
+HostStaging& thread_staging();
 
 // Copies bytes from device memory src to pageable host memory dst on stream s: the transfers land
 // in the pinned pieces (double-buffered) and host threads copy each piece on while the next one
 // transfers. Returns when dst holds every byte.
 void copy_to_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
-// The reverse: bytes of pageable host memory src into device memory dst on stream s, host threads
-// filling one pinned piece while the other transfers. src may be reused on return.
-void copy_from_pageable(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // Whether p is page-locked host memory (copied by DMA directly, not through the staging).
 bool is_pinned(const void* p);
 

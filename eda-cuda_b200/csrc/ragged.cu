@@ -183,9 +183,7 @@ std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_devic
   auto work = [&] {
     cudaStream_t ws = nullptr;
     Workspace* leased = nw > 1 ? lease_workspace() : nullptr;  // one worker: the caller's own
-    HostStaging* staging = nw > 1 ? lease_staging() : nullptr;
     if (leased) set_thread_workspace(leased);
-    if (staging) set_thread_staging(staging);
     try {
       EDAB_CUDA(cudaSetDevice(device));
       EDAB_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
@@ -210,10 +208,6 @@ std::unique_ptr<RaggedRun> decompose_ragged(const void* const* xs, bool on_devic
     if (leased) {
       set_thread_workspace(nullptr);
       return_workspace(leased);
-    }
-    if (staging) {
-      set_thread_staging(nullptr);
-      return_staging(staging);
     }
   };
   if (nw == 1) {

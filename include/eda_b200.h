@@ -180,7 +180,7 @@ EDA_API int eda_device_info(int device, char* buf, size_t len);
 
 /* Frees the calling thread's device workspace and its pinned host staging of device-to-host copies
  * (the reference's Context::release_unused_memory, cpp/src/runtime/context.cpp:154-160), and the
- * idle workspaces and pinned stagings that ragged-batch workers keep between calls. */
+ * idle workspaces that ragged-batch workers keep between calls. */
 EDA_API int eda_release_workspace(void);
 
 /* Device buffers for results returned to callers without an array library (the reference's output
