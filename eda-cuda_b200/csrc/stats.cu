@@ -255,6 +255,15 @@ __device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t digit, bool
 // items. cap keys per element; a selection with more candidates reads the items in every pass (the
 // count n keeps growing past cap, nothing is written there). 32-bit selections (three digits) have
 // no pass after the third and take none.
+// The digit pass that writes the candidates (the last passes read them): the third for 64-bit keys;
+// 32-bit keys (three digits) take candidates only where built with EDAB_SEL_CAND32 (written in the
+// second pass, after one digit: a quarter binade of the values).
+#ifndef EDAB_SEL_CAND32
+#define EDAB_SEL_CAND32 0
+#endif
+template <class K>
+constexpr int kCandPass = sizeof(K) == 8 ? 2 : 1;
+
 template <class K>
 struct SelCand {
   K* keys;               // [B][cap]; nullptr: no candidates
@@ -386,7 +395,7 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
     if (!live) break;
     const bool two = pass > 0 && !L->same;
     const K p0 = L->prefix[0], p1 = L->prefix[1];
-    if (pass == 3 && cand.keys) {  // the third pass's candidates are complete (the barrier above)
+    if (pass == kCandPass<K> + 1 && cand.keys) {  // the candidates are complete (the barrier above)
       const unsigned long long nc = *reinterpret_cast<volatile unsigned long long*>(cand.n + b);
       from_cand = nc <= static_cast<unsigned long long>(cand.cap);
       if (from_cand) n_it = static_cast<int64_t>(nc);
@@ -408,7 +417,7 @@ __global__ void __launch_bounds__(kThreads) select_cluster(Geom g, SelView<T> a,
       const K top = pass == 0 ? K(0) : (k >> hi);
       count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
       if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
-      if (pass == 2 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
+      if (pass == kCandPass<K> && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
     }
     __syncthreads();
     const int bins = 1 << width;
@@ -514,10 +523,10 @@ __global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T>
   const int tid = threadIdx.x;
   for (int i = tid; i < 2 * kDigitBins; i += kThreads) local[i] = 0u;
   __syncthreads();
-  // from the fourth pass on, the third pass's candidates (when they fit) instead of the items
+  // after the candidates pass, its candidates (when they fit) instead of the items
   bool from_cand = false;
   int64_t n_it = a.items;
-  if (pass >= 3 && cand.keys) {
+  if (pass > kCandPass<K> && cand.keys) {
     const unsigned long long nc = cand.n[b];
     from_cand = nc <= static_cast<unsigned long long>(cand.cap);
     if (from_cand) n_it = static_cast<int64_t>(nc);
@@ -537,7 +546,7 @@ __global__ void __launch_bounds__(kThreads) select_grid_count(Geom g, SelView<T>
     const K top = pass == 0 ? K(0) : (k >> hi);
     count_digit(local, digit, have && (pass == 0 || top == (p0 >> hi)));
     if (two) count_digit(local + kDigitBins, digit, have && top == (p1 >> hi));
-    if (pass == 2 && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
+    if (pass == kCandPass<K> && cand.keys) cand_append(cand, b, have && (top == (p0 >> hi) || (two && top == (p1 >> hi))), k);
   }
   __syncthreads();
   const int bins = 1 << width;
@@ -684,7 +693,7 @@ void select_grid(cudaStream_t s, const Geom& g, const SelView<T>& a, double q, c
   const int64_t fill = std::min<int64_t>((int64_t{8} * sms + g.batch - 1) / g.batch,
                                          std::max<int64_t>(1, a.items / (int64_t{kThreads} * 4)));
   const unsigned ctas = static_cast<unsigned>(std::clamp<int64_t>(std::max(by_items, fill), 1, 1024));
-  const SelCand<K> cand = sizeof(K) == 8 ? cand_of<K>(g, scratch) : SelCand<K>{};
+  const SelCand<K> cand = (sizeof(K) == 8 || EDAB_SEL_CAND32) ? cand_of<K>(g, scratch) : SelCand<K>{};
   if (cand.keys) EDAB_CUDA(cudaMemsetAsync(cand.n, 0, static_cast<size_t>(g.batch) * sizeof(unsigned long long), s));
   for (int pass = 0; pass < kDigits; ++pass) {
     select_grid_count<T, K><<<dim3(ctas, static_cast<unsigned>(g.batch)), kThreads, 0, s>>>(g, a, run, st, table, pass,
@@ -752,7 +761,7 @@ void select(cudaStream_t s, const Geom& g, const Sel<T>& sel, double q, const in
   };
   if constexpr (std::is_same_v<T, float>) {
     if (sel.center == nullptr) {
-      launch(select_cluster<T, uint32_t>, SelCand<uint32_t>{});
+      launch(select_cluster<T, uint32_t>, (EDAB_SEL_CAND32 && scratch) ? cand_of<uint32_t>(g, scratch) : SelCand<uint32_t>{});
       return;
     }
   }
