@@ -299,7 +299,8 @@ def run_ours(args) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps,
-        "step_ms": {"min": min(ms), "median": statistics.median(ms), "max": max(ms)} if ms else None,
+        "step_ms": {"min": min(ms), "median": statistics.median(ms), "max": max(ms),
+                    "all": [round(v, 3) for v in ms]} if ms else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"2-D {batch} x {SIDE}x{SIDE} float32 images per GPU (rings, wavy stripes, blobs, "
