@@ -296,10 +296,10 @@ def test_select_in_clusters(dev, dtype, shape):
                 assert cnt[b] == v.size
 
 
-# From the fourth digit on, a 64-bit selection (float64 items, or centred ones) reads the third
-# pass's candidates (the keys that share the first two digits) when they fit a quarter of the
-# items, else the items again: a constant field overflows the candidates, fields of one or many
-# binades do not. Both forms.
+# After its candidates' pass a selection reads the candidates (64-bit keys: the keys that share the
+# first two digits, read from the fourth pass; 32-bit keys: the first digit, read in the third) when
+# they fit a quarter of the items, else the items again: a constant field overflows the candidates,
+# a field of many binades does not, one binade lies near the limit. Both forms.
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("batch", [2, 40])
 def test_select_candidates_and_their_overflow(dev, dtype, batch):
