@@ -454,6 +454,15 @@ def run_other(args) -> None:
 
     dev = torch.device("cuda", 0)
     desc, data, axes, elements = other_workload(args.workload, 2024)
+    if args.length_class is not None:  # one length class of a ragged 1-D workload (profiling)
+        if axes is not None or data[0].ndim != 1:
+            raise SystemExit("--length-class applies to the ragged 1-D workloads")
+        k = args.length_class
+        data = [x for x in data if (1 << k) <= x.size < (2 << k)]
+        if not data:
+            raise SystemExit(f"no signal of the workload has a length in [2^{k}, 2^{k + 1})")
+        desc += f"; only the {len(data)} signals of lengths [2^{k}, 2^{k + 1})"
+        elements = len(data)
     ragged = axes is None
     if ragged:
         eda.set_length_classes(not args.exact_lengths)
@@ -584,6 +593,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end loop (profiling runs)")
     ap.add_argument("--workers", type=int, default=8,
                     help="concurrent shape groups of the ragged workloads (host threads with their own streams)")
+    ap.add_argument("--length-class", type=int, default=None, metavar="K",
+                    help="ragged 1-D workloads: only the signals of lengths [2^K, 2^(K+1)) (profiling one class)")
     ap.add_argument("--exact-lengths", action="store_true",
                     help="ragged 1-D workloads: group the signals by exact length instead of length class")
     ap.add_argument("--tune", action="store_true",
