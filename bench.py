@@ -494,10 +494,10 @@ def run_other(args) -> None:
             ms.append(e0.elapsed_time(e1))
     finally:
         clk.__exit__(None, None, None)
-    for _ in range(args.warmup):
+    for _ in range(0 if args.no_e2e else args.warmup):
         call_host()
     wall, d2h = [], 0
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         out = call_host()
@@ -549,7 +549,8 @@ def run_other(args) -> None:
                    **({"workers": args.workers,
                        "grouping": "exact shapes" if args.exact_lengths or data[0].ndim > 1 else "1-D length classes"}
                       if ragged else {})},
-        "e2e": {"value": elements * args.steps / (sum(wall) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": elements * args.steps / (sum(wall) / 1000.0) if wall else None, "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
         "fp64_err": err,
