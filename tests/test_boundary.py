@@ -146,3 +146,24 @@ def test_strided_argument_rules(case, message):
     buf = ctypes.create_string_buffer(512)
     lib.eda_last_error(buf, 512)
     assert message in buf.value.decode()
+
+
+def test_length_classes_setting_round_trips():
+    """How ragged 1-D batches group their signals is a process-wide host setting (no GPU needed)."""
+    import eda
+
+    assert eda.length_classes() is True  # the default
+    try:
+        eda.set_length_classes(False)
+        assert eda.length_classes() is False
+    finally:
+        eda.set_length_classes(True)
+    assert eda.length_classes() is True
+
+
+def test_ragged_collect_all_rejects_a_null_run():
+    from eda import _native
+
+    lib = _native.core()._lib
+    st = lib.eda_ragged_collect_all(None, None, 0, None, None)
+    assert st != 0
