@@ -973,6 +973,17 @@ __device__ __forceinline__ void reflect_span(int32_t u, int32_t v, int32_t n, in
   *hi = h;
 }
 
+// Whether the tiles of a line fold window q in shared memory of smem_elems samples: by bounds of any
+// tile's samples, slots and totals (nv, nx <= L + 2r + 2wa + 4, TS <= ((L + 2wa) / wa + 2) cps, checked
+// against every tile's exact extents on the CPU), so that every tile of a line, and the kernels of
+// the wider windows, decide alike.
+// Windows of one-chunk segments (cps 1) fold without chunk totals and always fit.
+__device__ __forceinline__ bool long_tiled(const Win& q, int32_t smem_elems) {
+  const int32_t span16 = (kLongTile + 2 * q.r + 2 * q.wa + 4 + 3) & ~3;
+  const int32_t ts_bound = q.cps == 1 ? 0 : ((kLongTile + 2 * q.wa) / q.wa + 2) * q.cps;
+  return 2 * span16 + 2 * ts_bound <= smem_elems;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a, const T* __restrict__ keys,
                                                          int32_t smem_elems) {
@@ -1009,88 +1020,304 @@ __global__ void __launch_bounds__(kCubeThreads) cube_long(Geom g, PassArgs<T> a,
   const int32_t xlo = min(max(gs, q.r) - q.r, n - 1 + q.r - he);
   const int32_t xhi = max(ge - q.r, n - 1 + q.r - max(hs, q.r));
   const int32_t nv = vhi - vlo + 1, nx = xhi - xlo + 1;
-  const int32_t TS = max(t.gn, t.hn) * q.cps;
+  const int32_t TS = q.cps == 1 ? 0 : max(t.gn, t.hn) * q.cps;  // one-chunk segments use no totals
   const int32_t nv16 = (nv + 3) & ~3, nx16 = (nx + 3) & ~3;  // 16-byte aligned regions
-  // Every tile of the line decides alike (a tile that folded alone beside a whole-line fold would
-  // rewrite the outputs that fold works in): by bounds of any tile's samples, slots and totals
-  // (nv, nx <= L + 2r + 2wa + 4, TS <= ((L + 2wa) / wa + 2) cps, checked against every tile's
-  // exact extents on the CPU).
-  const int32_t span16 = (kLongTile + 2 * q.r + 2 * q.wa + 4 + 3) & ~3;
-  const int32_t ts_bound = ((kLongTile + 2 * q.wa) / q.wa + 2) * q.cps;
-  const bool tiled = 2 * span16 + 2 * ts_bound <= smem_elems && nv16 + nx16 + 2 * TS <= smem_elems;
-  if (!tiled && blockIdx.x != 0) return;  // the whole line folds in the tile-0 CTA
+  // wider windows fold in the segment kernels below (every tile of the line decides alike); the
+  // exact extents lie within the bounds (a tile past them would return, no access outside)
+  if (!long_tiled(q, smem_elems) || nv16 + nx16 + 2 * TS > smem_elems) return;
   __syncthreads();
   const T* line = keys + b * g.pitch;
   unsigned long long acct = 0;
-  if (tiled) {
-    T* Vs = reinterpret_cast<T*>(smem_raw);
-    T* Rs = Vs + nv16;
-    T* tot = Rs + nx16;
-    for (int32_t i = threadIdx.x; i < nv; i += blockDim.x) Vs[i] = line[vlo + i];
-    __syncthreads();
-    for (int f = 0; f < nf; ++f) {
-      const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-      // (the staged samples and slots at their line indices: only the staged ones are touched)
-      if (box) run_stage<T, kOpSum, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
-      else if (is_min) run_stage<T, kOpMinK, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
-      else run_stage<T, kOpMaxK, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
-      T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
-      const T* aux = detsq ? a.aux + b * g.field : nullptr;
-      const int32_t end = X1 == n ? static_cast<int32_t>(g.pitch) : X1;  // the last tile writes the pads
-      for (int32_t x = X0 + threadIdx.x; x < end; x += blockDim.x) {
-        T y = T(0);
-        if (x < n) {
-          y = Rs[x - xlo];
-          if (!box) {
-            y = okey(y);
-          } else if (a.last) {
-            y = mul_rn(y, fac_s);
-            if (detsq) {
-              const T d = sub_rn(aux[x], y);
-              y = mul_rn(d, d);
-            }
+  T* Vs = reinterpret_cast<T*>(smem_raw);
+  T* Rs = Vs + nv16;
+  T* tot = Rs + nx16;
+  for (int32_t i = threadIdx.x; i < nv; i += blockDim.x) Vs[i] = line[vlo + i];
+  __syncthreads();
+  for (int f = 0; f < nf; ++f) {
+    const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
+    // (the staged samples and slots at their line indices: only the staged ones are touched)
+    if (box) run_stage<T, kOpSum, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+    else if (is_min) run_stage<T, kOpMinK, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+    else run_stage<T, kOpMaxK, 1, 1, true>(Vs - vlo, Rs - xlo, tot, n, TS, t, 0, a.seq_share);
+    T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
+    const T* aux = detsq ? a.aux + b * g.field : nullptr;
+    const int32_t end = X1 == n ? static_cast<int32_t>(g.pitch) : X1;  // the last tile writes the pads
+    for (int32_t x = X0 + threadIdx.x; x < end; x += blockDim.x) {
+      T y = T(0);
+      if (x < n) {
+        y = Rs[x - xlo];
+        if (!box) {
+          y = okey(y);
+        } else if (a.last) {
+          y = mul_rn(y, fac_s);
+          if (detsq) {
+            const T d = sub_rn(aux[x], y);
+            y = mul_rn(d, d);
           }
         }
-        R[x] = y;
       }
-      __syncthreads();  // the next field rewrites the slots and totals
+      R[x] = y;
     }
-    acct = static_cast<unsigned long long>(X1 - X0) * sizeof(T) * (1 + nf);
-  } else {
-    T* tot = reinterpret_cast<T*>(smem_raw);
-    const int32_t TSL = tot_slots(n);
-    for (int f = 0; f < nf; ++f) {
-      T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(j) * a.out_stride + b * g.field;
-      const bool is_min = a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1);
-      if (box) run_stage<T, kOpSum, 1, 1>(line, R, tot, n, TSL, q, 0, a.seq_share);
-      else if (is_min) run_stage<T, kOpMinK, 1, 1>(line, R, tot, n, TSL, q, 0, a.seq_share);
-      else run_stage<T, kOpMaxK, 1, 1>(line, R, tot, n, TSL, q, 0, a.seq_share);
-      // the epilogue in place (run_stage ended on a barrier: every output is written); pads are 0
-      const T* aux = detsq ? a.aux + b * g.field : nullptr;
-      for (int32_t i = threadIdx.x; i < static_cast<int32_t>(g.pitch); i += blockDim.x) {
-        T y = i < n ? R[i] : T(0);
-        if (i < n) {
-          if (!box) {
-            y = okey(y);
-          } else if (a.last) {
-            y = mul_rn(y, fac_s);
-            if (detsq) {
-              const T d = sub_rn(aux[i], y);
-              y = mul_rn(d, d);
-            }
-          }
-        }
-        R[i] = y;
-      }
-      __syncthreads();
-    }
-    acct = static_cast<unsigned long long>(n) * sizeof(T) * (1 + nf);
+    __syncthreads();  // the next field rewrites the slots and totals
   }
+  acct = static_cast<unsigned long long>(X1 - X0) * sizeof(T) * (1 + nf);
   if (a.bytes && threadIdx.x == 0) atomicAdd(a.bytes, acct);
+}
+
+// The windows too wide for the tiles (their segments exceed a tile's shared memory) fold each line
+// in four launches over many CTAs, with no CTA waiting for another: the chunk totals of both
+// directions into a global table, the per-segment exclusive carries, the H folds into the output
+// row, the G folds combined with them; then the pass's epilogue. The tasks and their arithmetic are
+// those of the staged kernel's chunk schedule (one lane per chunk of a line), so every bit is the
+// same. tot: per field, rung and element 2 x TSL samples (TSL = tot_slots of the longest line).
+struct LongSeg {
+  int64_t b;
+  int32_t j, n, e_max;
+  Win q;
+  bool wide;  // the window folds here (not in the tiles)
+};
+template <class T>
+__device__ __forceinline__ LongSeg long_seg(const Geom& g, const PassArgs<T>& a, int32_t smem_elems) {
+  LongSeg L{};
+  L.b = blockIdx.y;
+  L.j = static_cast<int32_t>(blockIdx.z);
+  L.n = elem_len(g, L.b);
+  const int32_t w = a.win[static_cast<int64_t>(L.j) * g.batch + L.b];
+  if (w < 1) return L;
+  L.q = make_win(L.n, w);
+  L.e_max = L.n - 1 + L.q.r;
+  // (a wide window has segments of many chunks: nseg cps <= tot_slots(n) <= TSL, checked on the CPU
+  // for every length and window; the kernels also leave any other window alone)
+  L.wide = !long_tiled(L.q, smem_elems) && L.q.cps > 1 && L.q.nseg * L.q.cps <= tot_slots(L.n);
+  return L;
+}
+template <class T>
+__device__ __forceinline__ int op_of(const PassArgs<T>& a, int f) {
+  if (a.op == static_cast<int>(CubeOp::kBox)) return kOpSum;
+  return (a.op == static_cast<int>(CubeOp::kMin) || (a.op == static_cast<int>(CubeOp::kMaxMin) && f == 1)) ? kOpMinK
+                                                                                                          : kOpMaxK;
+}
+
+// Chunk totals: task t < 2 nseg cps is (direction, segment, chunk), the line's G chunks first.
+template <class T, int OP>
+__device__ __forceinline__ void seg_totals(const LongSeg& L, const T* __restrict__ V, T* __restrict__ tot, int32_t TS) {
+  const Win& q = L.q;
+  const int32_t per_dir = q.nseg * q.cps;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < 2 * per_dir; t += stride) {
+    const int dir = t >= per_dir;
+    const int32_t kc = static_cast<int32_t>(t - dir * per_dir);
+    const int32_t k = kc / q.cps, c = kc - k * q.cps;
+    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t e_last = min(s + q.wa - 1, L.e_max);
+    const int32_t c0 = s + 32 * c;
+    if (c0 > e_last) continue;
+    const int32_t c1 = min(c0 + 31, e_last);
+    const int32_t n = L.n;
+    T total;
+    if (c0 >= 0 && c1 <= n - 1) {
+      if (dir) {
+        const T* vp = V + (n - 1 - c0);
+        total = c1 == c0 + 31 ? chunk_total<T, OP, -1>(vp) : partial_total<T, OP, -1>(vp, c1 - c0 + 1);
+      } else {
+        const T* vp = V + c0;
+        total = c1 == c0 + 31 ? chunk_total<T, OP, 1>(vp) : partial_total<T, OP, 1>(vp, c1 - c0 + 1);
+      }
+    } else {
+      total = fold_chunk<T, OP>(V, 1, n, c0, c1, dir, [](int32_t, T) {});
+    }
+    tot[dir * TS + kc] = total;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) long_totals(Geom g, PassArgs<T> a, const T* __restrict__ keys, int f,
+                                                        T* tot_all, int32_t TSL, int32_t smem_elems) {
+  const LongSeg L = long_seg(g, a, smem_elems);
+  if (!L.wide) return;
+  const T* V = keys + L.b * g.pitch;
+  T* tot = tot_all + ((static_cast<int64_t>(L.j) * g.batch + L.b) * 2) * TSL;
+  const int op = op_of(a, f);
+  if (op == kOpSum) seg_totals<T, kOpSum>(L, V, tot, TSL);
+  else if (op == kOpMinK) seg_totals<T, kOpMinK>(L, V, tot, TSL);
+  else seg_totals<T, kOpMaxK>(L, V, tot, TSL);
+}
+
+// Exclusive carries per segment and direction, in place (slot c holds the carry of chunk c >= 1),
+// sequential in chunk order (the canonical carries of sums), from shared memory.
+template <class T>
+__global__ void __launch_bounds__(kThreads) long_carries(Geom g, PassArgs<T> a, int f, T* tot_all, int32_t TSL,
+                                                         int32_t smem_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const LongSeg L = long_seg(g, a, smem_elems);
+  if (!L.wide) return;
+  const Win& q = L.q;
+  T* tot = tot_all + ((static_cast<int64_t>(L.j) * g.batch + L.b) * 2) * TSL;
+  T* st = reinterpret_cast<T*>(smem_raw);  // [2][nseg cps]
+  const int32_t per_dir = q.nseg * q.cps;
+  for (int32_t i = threadIdx.x; i < 2 * per_dir; i += blockDim.x) {
+    const int dir = i >= per_dir;
+    st[i] = tot[dir * TSL + (i - dir * per_dir)];
+  }
+  __syncthreads();
+  const int op = op_of(a, f);
+  for (int32_t t = threadIdx.x; t < 2 * q.nseg; t += blockDim.x) {
+    const int dir = t >= q.nseg;
+    const int32_t k = t - dir * q.nseg;
+    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t e_last = min(s + q.wa - 1, L.e_max);
+    const int32_t nch = (e_last - s) / 32 + 1;
+    T* tl = st + dir * per_dir + k * q.cps;
+    T run = tl[0];
+    for (int32_t c = 1; c < nch; ++c) {
+      const T next = tl[c];
+      tl[c] = run;
+      run = op == kOpSum ? fop<kOpSum>(run, next) : (op == kOpMinK ? fop<kOpMinK>(run, next) : fop<kOpMaxK>(run, next));
+    }
+  }
+  __syncthreads();
+  for (int32_t i = threadIdx.x; i < 2 * per_dir; i += blockDim.x) {
+    const int dir = i >= per_dir;
+    tot[dir * TSL + (i - dir * per_dir)] = st[i];
+  }
+}
+
+// H (the reversed line's G) of task t = (segment, chunk) into the output slots n - 1 + r - e (e >= r).
+template <class T, int OP>
+__device__ __forceinline__ void seg_fold_h(const LongSeg& L, const T* __restrict__ V, T* __restrict__ R,
+                                           const T* __restrict__ tot, int32_t TS) {
+  const Win& q = L.q;
+  const int32_t n = L.n;
+  const T idn = fold_identity<T, OP>();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < q.nseg * q.cps; t += stride) {
+    const int32_t kc = static_cast<int32_t>(t);
+    const int32_t k = kc / q.cps, c = kc - k * q.cps;
+    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t e_last = min(s + q.wa - 1, L.e_max);
+    const int32_t c0 = s + 32 * c;
+    if (c0 > e_last) continue;
+    const int32_t c1 = min(c0 + 31, e_last);
+    const T cv = c > 0 ? tot[TS + kc] : idn;
+    if (c0 >= 0 && c1 <= n - 1) {
+      const T* vp = V + (n - 1 - c0);
+      T* rp = R + (n - 1 + q.r - c0);
+      if (c1 == c0 + 31 && c0 >= q.r) chunk_h<T, OP, 1>(vp, rp, cv);
+      else partial_h<T, OP, 1>(vp, rp, c1 - c0 + 1, max(0, q.r - c0), cv);
+    } else {
+      fold_chunk<T, OP>(V, 1, n, c0, c1, 1, [&](int32_t e, T loc) {
+        if (e >= q.r) R[n - 1 + q.r - e] = fop<OP>(cv, loc);
+      });
+    }
+  }
+}
+// G of task t combined with the H in its slots: y(x) = op(H(x - r), G(x + r)), slot x = e - r.
+template <class T, int OP>
+__device__ __forceinline__ void seg_fold_g(const LongSeg& L, const T* __restrict__ V, T* __restrict__ R,
+                                           const T* __restrict__ tot) {
+  const Win& q = L.q;
+  const int32_t n = L.n;
+  const T idn = fold_identity<T, OP>();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < q.nseg * q.cps; t += stride) {
+    const int32_t kc = static_cast<int32_t>(t);
+    const int32_t k = kc / q.cps, c = kc - k * q.cps;
+    const int32_t s = q.o + (q.k_lo + k) * q.wa;
+    const int32_t e_al = s + q.wa - 1;
+    const int32_t e_last = min(e_al, L.e_max);
+    const int32_t c0 = s + 32 * c;
+    if (c0 > e_last) continue;
+    const int32_t c1 = min(c0 + 31, e_last);
+    const T cv = c > 0 ? tot[kc] : idn;
+    if (c0 >= 0 && c1 <= n - 1) {
+      const T* vp = V + c0;
+      T* rp = R + (c0 - q.r);
+      if (c1 == c0 + 31 && c0 >= q.r) chunk_g<T, OP, 1>(vp, rp, cv, c1 == e_al);
+      else partial_g<T, OP, 1>(vp, rp, c1 - c0 + 1, max(0, q.r - c0), cv, c1 == e_al);
+    } else {
+      fold_chunk<T, OP>(V, 1, n, c0, c1, 0, [&](int32_t e, T loc) {
+        if (e < q.r) return;
+        const T gv = fop<OP>(cv, loc);
+        T* slot = R + (e - q.r);
+        const T h = *slot;
+        if constexpr (OP == kOpSum) {
+          const T sum = add_rn(h, gv);
+          *slot = e == e_al ? mul_rn(sum, T(0.5)) : sum;
+        } else {
+          *slot = fop<OP>(h, gv);
+        }
+      });
+    }
+  }
+}
+
+// pass H (G = false) or G (G = true) of field f over the wide windows
+template <class T, bool G>
+__global__ void __launch_bounds__(kThreads) long_folds(Geom g, PassArgs<T> a, const T* __restrict__ keys, int f,
+                                                       const T* tot_all, int32_t TSL, int32_t smem_elems) {
+  const LongSeg L = long_seg(g, a, smem_elems);
+  if (!L.wide) return;
+  const T* V = keys + L.b * g.pitch;
+  T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(L.j) * a.out_stride + L.b * g.field;
+  const T* tot = tot_all + ((static_cast<int64_t>(L.j) * g.batch + L.b) * 2) * TSL;
+  const int op = op_of(a, f);
+  if constexpr (G) {
+    if (op == kOpSum) seg_fold_g<T, kOpSum>(L, V, R, tot);
+    else if (op == kOpMinK) seg_fold_g<T, kOpMinK>(L, V, R, tot);
+    else seg_fold_g<T, kOpMaxK>(L, V, R, tot);
+  } else {
+    if (op == kOpSum) seg_fold_h<T, kOpSum>(L, V, R, tot, TSL);
+    else if (op == kOpMinK) seg_fold_h<T, kOpMinK>(L, V, R, tot, TSL);
+    else seg_fold_h<T, kOpMaxK>(L, V, R, tot, TSL);
+  }
+}
+
+// The pass's epilogue on the folded row of field f (order keys back to values; the box's scale and
+// detail energy on its last pass); the pads are written 0.
+template <class T>
+__global__ void __launch_bounds__(kThreads) long_epilogue(Geom g, PassArgs<T> a, int f, int32_t smem_elems) {
+  const LongSeg L = long_seg(g, a, smem_elems);
+  if (!L.wide) return;
+  const bool box = a.op == static_cast<int>(CubeOp::kBox);
+  const bool detsq = box && a.last && a.epi == static_cast<int>(BoxEpi::kDetSq);
+  const T fac = static_cast<T>(1.0 / static_cast<double>(L.q.wa));
+  T* R = (f == 0 ? a.out0 : a.out1) + static_cast<int64_t>(L.j) * a.out_stride + L.b * g.field;
+  const T* aux = detsq ? a.aux + L.b * g.field : nullptr;
+  const int32_t pitch = static_cast<int32_t>(g.pitch);
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pitch; i += gridDim.x * blockDim.x) {
+    T y = T(0);
+    if (i < L.n) {
+      y = R[i];
+      if (!box) {
+        y = okey(y);
+      } else if (a.last) {
+        y = mul_rn(y, fac);
+        if (detsq) {
+          const T d = sub_rn(aux[i], y);
+          y = mul_rn(d, d);
+        }
+      }
+    }
+    R[i] = y;
+  }
+  if (a.bytes && f == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
+    atomicAdd(a.bytes, static_cast<unsigned long long>(L.n) * sizeof(T) * (1 + nf));
+  }
 }
 
 thread_local void* t_long_scratch = nullptr;
 thread_local size_t t_long_bytes = 0;
+
+// The long-line scratch: the lines' fold input (batch x pitch samples), then the wide windows' chunk
+// totals (rungs x batch x 2 x tot_slots(longest line) samples).
+size_t long_keys_bytes(const Geom& g, size_t es) {
+  return (static_cast<size_t>(g.batch) * static_cast<size_t>(g.pitch) * es + 255) / 256 * 256;
+}
+size_t long_scratch_need(const Geom& g, size_t es) {
+  return long_keys_bytes(g, es) +
+         static_cast<size_t>(kMaxRungs) * static_cast<size_t>(g.batch) * 2 * static_cast<size_t>(tot_slots(g.n_last)) * es;
+}
 
 size_t smem_bytes(int32_t n, int P, bool rows, size_t es, bool dbuf = true) {
   const int32_t gel = es == 4 ? group_elems<float>(n, P, rows) : group_elems<double>(n, P, rows);
@@ -1159,21 +1386,25 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 template <class T>
 void launch_long(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   if (g.dim != 1) throw std::invalid_argument("edab: lines beyond the shared-memory capacity are 1-D only");
-  const size_t need = static_cast<size_t>(g.batch) * static_cast<size_t>(g.pitch) * sizeof(T);
-  if (t_long_scratch == nullptr || t_long_bytes < need) {
+  const size_t keys_bytes = long_keys_bytes(g, sizeof(T));
+  const int32_t TSL = tot_slots(g.n_last);
+  if (t_long_scratch == nullptr || t_long_bytes < long_scratch_need(g, sizeof(T))) {
     throw std::logic_error("edab: a long-line cube pass needs the thread's long-line scratch");
   }
   T* keys = static_cast<T*>(t_long_scratch);
+  T* tot = reinterpret_cast<T*>(static_cast<unsigned char*>(t_long_scratch) + keys_bytes);
   long_line_input<T><<<blocks_for(g.batch * g.pitch), kThreads, 0, s>>>(g, a, keys);
   EDAB_LAUNCH("long_line_input");
-  // shared memory: the whole-line fold's chunk totals, and at least half an SM's (two tile CTAs per
-  // SM) for the tiles' samples, slots and totals
-  const size_t whole = static_cast<size_t>(2) * tot_slots(g.n_last) * sizeof(T);
+  // shared memory: a line's chunk totals (the wide windows' carries), and at least half an SM's (two
+  // tile CTAs per SM) for the tiles' samples, slots and totals
+  const size_t whole = static_cast<size_t>(2) * TSL * sizeof(T);
   if (whole > dev_facts().smem) throw std::invalid_argument("edab: a line is too long for the long-line cube pass");
   const size_t half_sm = (dev_facts().sm_smem / 2 - 2048) / 16 * 16;
   const size_t smem = std::min(dev_facts().smem, std::max(whole, half_sm)) / 16 * 16;
   once_on_device(reinterpret_cast<const void*>(cube_long<T>), [] {
     EDAB_CUDA(cudaFuncSetAttribute(cube_long<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(dev_facts().smem)));
+    EDAB_CUDA(cudaFuncSetAttribute(long_carries<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(dev_facts().smem)));
   });
   const int64_t tiles = (g.n_last + kLongTile - 1) / kLongTile;
@@ -1181,8 +1412,28 @@ void launch_long(cudaStream_t s, const Geom& g, PassArgs<T> a) {
   a.bytes = cube_bytes_counter();
   profile_cube_launch(s, true);
   const dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs));
-  cube_long<T><<<grid, kCubeThreads, smem, s>>>(g, a, keys, static_cast<int32_t>(smem / sizeof(T)));
+  const int32_t smem_elems = static_cast<int32_t>(smem / sizeof(T));
+  cube_long<T><<<grid, kCubeThreads, smem, s>>>(g, a, keys, smem_elems);
   EDAB_LAUNCH("cube_long");
+  // the wide windows (the kernels return at once for the windows the tiles took)
+  const int nf = a.op == static_cast<int>(CubeOp::kMaxMin) ? 2 : 1;
+  const unsigned xt = static_cast<unsigned>(std::clamp<int64_t>((TSL + kThreads - 1) / kThreads, 1, 32));
+  const unsigned xe = static_cast<unsigned>(std::clamp<int64_t>((g.pitch + 4 * kThreads - 1) / (4 * kThreads), 1, 16));
+  const dim3 gt(xt, static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs));
+  const dim3 g1(1, static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs));
+  const dim3 ge(xe, static_cast<unsigned>(g.batch), static_cast<unsigned>(a.rungs));
+  for (int f = 0; f < nf; ++f) {
+    long_totals<T><<<gt, kThreads, 0, s>>>(g, a, keys, f, tot, TSL, smem_elems);
+    EDAB_LAUNCH("long_totals");
+    long_carries<T><<<g1, kThreads, whole, s>>>(g, a, f, tot, TSL, smem_elems);
+    EDAB_LAUNCH("long_carries");
+    long_folds<T, false><<<gt, kThreads, 0, s>>>(g, a, keys, f, tot, TSL, smem_elems);
+    EDAB_LAUNCH("long_folds");
+    long_folds<T, true><<<gt, kThreads, 0, s>>>(g, a, keys, f, tot, TSL, smem_elems);
+    EDAB_LAUNCH("long_folds");
+    long_epilogue<T><<<ge, kThreads, 0, s>>>(g, a, f, smem_elems);
+    EDAB_LAUNCH("long_epilogue");
+  }
   profile_cube_launch(s, false);
 }
 
@@ -1310,7 +1561,7 @@ size_t long_line_scratch_bytes(const Geom& g, size_t es) {
   if (g.dim != 1) return 0;
   const size_t staged = es == 4 ? smem_bytes(g.n_last, 1, true, 4) : smem_bytes(g.n_last, 1, true, 8);
   if (staged <= dev_facts().smem) return 0;
-  return static_cast<size_t>(g.batch) * static_cast<size_t>(g.pitch) * es;
+  return long_scratch_need(g, es);
 }
 
 template <class T>

@@ -98,4 +98,26 @@ def test_every_tile_within_the_shared_bounds():
         ts = max(q["gn"], q["hn"]) * q["cps"]
         bound = L + 2 * q["r"] + 2 * q["wa"] + 4
         assert nv <= bound and nx <= bound, (n, w, t)
-        assert ts <= ((L + 2 * q["wa"]) // q["wa"] + 2) * q["cps"], (n, w, t)
+        if q["cps"] > 1:  # one-chunk segments use no totals
+            assert ts <= ((L + 2 * q["wa"]) // q["wa"] + 2) * q["cps"], (n, w, t)
+
+
+def test_wide_windows_fit_the_chunk_table():
+    """Windows too wide for the tiles fold in separate launches whose chunk tasks (segment k, chunk
+    c) index a table of 2 x tot_slots(n) = 2 (n / 8 + 24) totals per line and rung, and whose carry
+    launch stages that table in shared memory: nseg cps must fit it for every length and window."""
+    rng = random.Random(11)
+    for _ in range(200000):
+        n = rng.randint(2, 65536)
+        w = 2 * rng.randint(0, rng.choice([20, 200, 5000, 70000])) + 1
+        r = min((w - 1) // 2, n - 1)
+        wa = 2 * r + 1
+        o = (n * ((wa + 1) // 2)) % wa
+        nseg = (n - 1 + r - o) // wa - (r - o) // wa + 1
+        cps = (wa + 31) >> 5
+        if cps == 1:  # one-chunk segments always fold in the tiles (even in the smallest budget, the
+            # 14 080 float64 samples of half an SM), so they never reach the chunk table
+            span16 = (L + 2 * r + 2 * wa + 4 + 3) & ~3
+            assert 2 * span16 <= 14080
+            continue
+        assert nseg * cps <= n // 8 + 24, (n, w, nseg, cps)
