@@ -938,10 +938,10 @@ __global__ void __launch_bounds__(kCubeThreads, EDAB_CUBE_CTAS) cube_pass(Geom g
 // stages the samples of the segments its outputs need (x - r lies in a segment of the reversed
 // line, whose H it folds; x + r in a segment of the line, whose G it folds; every segment whole,
 // from its start, so every fold is the canonical one) and runs the staged kernel's fold phases on
-// them in shared memory. A window whose segments do not fit a tile's shared memory folds the whole
-// line in one CTA (the tile-0 CTA; the other tiles return) on global memory (the line and its
-// output stay in L2), with the chunk totals in shared memory. Every bit of the result is that of
-// the staged kernel.
+// them in shared memory. A window whose segments do not fit a tile's shared memory folds in the
+// segment launches further down (chunk totals, carries, H and G folds over many CTAs, on global
+// memory: the line and its output stay in L2). Every bit of the result is that of the staged
+// kernel.
 template <class T>
 __global__ void __launch_bounds__(kThreads) long_line_input(Geom g, PassArgs<T> a, T* keys) {
   const int64_t total = g.batch * g.pitch;  // 1-D: one row per element
